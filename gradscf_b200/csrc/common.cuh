@@ -1,0 +1,266 @@
+// Shared device code: class traits, Cartesian component tables, the Boys
+// function and Rys roots/weights (tables generated by gen_tables.py).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define B200JK_PI 3.14159265358979323846
+// 2 pi^(5/2): prefactor of the (ss|ss) integral, 2 pi^2.5 / (p q sqrt(p+q)).
+#define B200JK_ERI_C0 34.98683665524972497
+
+namespace b200jk {
+
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+
+// Cartesian component ordering of libcint: lx descending, then ly descending
+// (xx, xy, xz, yy, yz, zz for d).  Index i of shell l -> exponents.
+__host__ __device__ constexpr int cart_lx(int l, int i) {
+  int lx = l, k = i;
+  while (k > l - lx) { k -= l - lx + 1; --lx; }
+  return lx;
+}
+__host__ __device__ constexpr int cart_ly(int l, int i) {
+  int lx = l, k = i;
+  while (k > l - lx) { k -= l - lx + 1; --lx; }
+  return l - lx - k;
+}
+__host__ __device__ constexpr int cart_lz(int l, int i) {
+  return l - cart_lx(l, i) - cart_ly(l, i);
+}
+
+template <int LA, int LB, int LC, int LD>
+struct ClassInfo {
+  static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  static constexpr int NAB = NA * NB, NCD = NC * ND, NOUT = NAB * NCD;
+  static constexpr int LAB = LA + LB, LCD = LC + LD, L = LAB + LCD;
+  static constexpr int NROOT = L / 2 + 1;
+  static constexpr int NG = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
+  static constexpr int NV = (LAB + 1) * (LCD + 1);
+};
+
+__host__ __device__ constexpr int binom(int n, int k) {
+  int r = 1;
+  for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+  return r;
+}
+
+template <typename R> __device__ __forceinline__ R dexp(R x);
+template <> __device__ __forceinline__ double dexp<double>(double x) { return exp(x); }
+template <> __device__ __forceinline__ float dexp<float>(float x) { return __expf(x); }
+template <typename R> __device__ __forceinline__ R dsqrt(R x);
+template <> __device__ __forceinline__ double dsqrt<double>(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float dsqrt<float>(float x) { return sqrtf(x); }
+template <typename R> __device__ __forceinline__ R drsqrt(R x);
+template <> __device__ __forceinline__ double drsqrt<double>(double x) { return rsqrt(x); }
+template <> __device__ __forceinline__ float drsqrt<float>(float x) { return rsqrtf(x); }
+
+// Device-resident lookup tables (see gen_tables.py for their definition).
+struct Tables {
+  const double* rys;        // Chebyshev coefficients, [n][interval][coef][2n]
+  const float* rys_f;       // same, float
+  const int* rys_off;       // offset of each n in rys
+  const int* rys_nint;      // number of tabulated unit intervals per n
+  const double* asym_r;     // [n][RYS_MAX_N] large-T root numerators s_i^2
+  const double* asym_w;     // [n][RYS_MAX_N] large-T weight numerators h_i
+  const double* boys;       // [row][col] F_col(row / BOYS_STEP_INV)
+  const float* boys_f;
+  const double* c2s;        // per l: [kTW][kTW] output transform (cart->sph or cart factor)
+};
+
+// Output-transform table layout: per l a kTW x kTW block, row = raw Cartesian
+// component, column = output function (up to 10 for Cartesian f).
+constexpr int kTW = 10;
+constexpr int kTS = kTW * kTW;
+
+// Boys function F_0..F_M(T) into f[0..M], M <= 8.
+// T < 40: 8-term Taylor expansion of F_M about the nearest grid point
+// (spacing 1/20) followed by the stable downward recursion
+//   F_m = (2 T F_{m+1} + e^{-T}) / (2m + 1).
+// T >= 40: F_0 = sqrt(pi/T)/2 and the stable upward recursion
+//   F_{m+1} = ((2m+1) F_m - e^{-T}) / (2T).
+// (Taylor/downward scheme: Gill, Johnson & Pople, Int. J. Quantum Chem. 40, 745 (1991).)
+template <int M, typename R>
+__device__ __forceinline__ void boys_fn(R t, R* f, const R* grid) {
+  constexpr int NCOL = 24;       // BOYS_MMAX + BOYS_TERMS
+  if (t < R(40)) {
+    const int k = min(max(__float2int_rn(float(t) * 20.0f), 0), 800);
+    const R dt = R(k) * R(0.05) - t;          // -(t - t_k)
+    const R* row = grid + k * NCOL + M;
+    R acc = row[7];
+#pragma unroll
+    for (int i = 6; i >= 0; --i) acc = row[i] + acc * dt / R(i + 1);
+    f[M] = acc;
+    if (M > 0) {
+      const R e = dexp<R>(-t);
+#pragma unroll
+      for (int m = M - 1; m >= 0; --m) f[m] = (R(2) * t * f[m + 1] + e) / R(2 * m + 1);
+    }
+  } else {
+    const R e = dexp<R>(-t);
+    f[0] = R(0.886226925452758014) * drsqrt<R>(t);   // sqrt(pi)/2 / sqrt(t)
+    const R inv2t = R(0.5) / t;
+#pragma unroll
+    for (int m = 0; m < M; ++m) f[m + 1] = (R(2 * m + 1) * f[m] - e) * inv2t;
+  }
+}
+
+// Rys nodes x_i = t_i^2 and weights w_i for N <= 2 from the Boys moments
+// mu_k = F_k(T): Chebyshev algorithm for the recurrence coefficients, then
+// the 1x1 / 2x2 Jacobi eigenproblem in closed form.
+template <int N, typename R>
+__device__ __forceinline__ void rys_small(R t, R* x, R* w, const R* grid) {
+  if (N == 1) {
+    R f[2];
+    boys_fn<1, R>(t, f, grid);
+    w[0] = f[0];
+    x[0] = f[1] / f[0];
+  } else {
+    R f[4];
+    boys_fn<3, R>(t, f, grid);
+    const R a0 = f[1] / f[0];
+    const R s11 = f[2] - a0 * f[1];
+    const R s12 = f[3] - a0 * f[2];
+    const R a1 = s12 / s11 - a0;
+    const R b1 = s11 / f[0];
+    const R mid = R(0.5) * (a0 + a1), hd = R(0.5) * (a0 - a1);
+    const R rad = dsqrt<R>(hd * hd + b1);
+    const R xp = mid + rad;
+    const R xm = (a0 * a1 - b1) / xp;          // product of the roots / larger root
+    x[0] = xm;
+    x[1] = xp;
+    const R dm = xm - a0, dp = xp - a0;
+    w[0] = f[0] * b1 / (b1 + dm * dm);
+    w[1] = f[0] * b1 / (b1 + dp * dp);
+  }
+}
+
+// One Rys function (root or weight index fidx of N) from the Chebyshev table.
+template <typename R>
+__device__ __forceinline__ R rys_cheb(const R* tab, int off, int nfun, int fidx, int interval, R s) {
+  const R* c = tab + off + interval * 12 * nfun + fidx;
+  R b1 = R(0), b2 = R(0);
+  const R s2 = s + s;
+#pragma unroll
+  for (int k = 11; k >= 1; --k) {
+    const R b0 = c[k * nfun] + s2 * b1 - b2;
+    b2 = b1;
+    b1 = b0;
+  }
+  return c[0] + s * b1 - b2;
+}
+
+template <typename R> struct TableSel;
+template <> struct TableSel<double> {
+  static __device__ __forceinline__ const double* rys(const Tables& t) { return t.rys; }
+  static __device__ __forceinline__ const double* boys(const Tables& t) { return t.boys; }
+};
+template <> struct TableSel<float> {
+  static __device__ __forceinline__ const float* rys(const Tables& t) { return t.rys_f; }
+  static __device__ __forceinline__ const float* boys(const Tables& t) { return t.boys_f; }
+};
+
+// All N nodes/weights by one thread.
+template <int N, typename R>
+__device__ __forceinline__ void rys_roots(R t, R* x, R* w, const Tables& tb) {
+  if (N <= 2) {
+    rys_small<N, R>(t, x, w, TableSel<R>::boys(tb));
+    return;
+  }
+  const int nint = tb.rys_nint[N];
+  if (t >= R(nint)) {
+    const R rt = R(1) / t, rs = drsqrt<R>(t);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      x[i] = R(tb.asym_r[N * 8 + i]) * rt;
+      w[i] = R(tb.asym_w[N * 8 + i]) * rs;
+    }
+    return;
+  }
+  const int k = min(max(int(t), 0), nint - 1);
+  const R s = R(2) * (t - R(k)) - R(1);
+  const R* tab = TableSel<R>::rys(tb);
+  const int off = tb.rys_off[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    x[i] = rys_cheb<R>(tab, off, 2 * N, i, k, s);
+    w[i] = rys_cheb<R>(tab, off, 2 * N, N + i, k, s);
+  }
+}
+
+// One of the 2N functions (index f: nodes 0..N-1 then weights) -- used when
+// several threads share one primitive quartet.
+template <int N, typename R>
+__device__ __forceinline__ R rys_one(R t, int f, const Tables& tb) {
+  if (N <= 2) {
+    R x[N], w[N];
+    rys_small<N, R>(t, x, w, TableSel<R>::boys(tb));
+    R v = x[0];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      if (f == i) v = x[i];
+      if (f == N + i) v = w[i];
+    }
+    return v;
+  }
+  const int nint = tb.rys_nint[N];
+  if (t >= R(nint)) {
+    if (f < N) return R(tb.asym_r[N * 8 + f]) / t;
+    return R(tb.asym_w[N * 8 + f - N]) * drsqrt<R>(t);
+  }
+  const int k = min(max(int(t), 0), nint - 1);
+  const R s = R(2) * (t - R(k)) - R(1);
+  return rys_cheb<R>(TableSel<R>::rys(tb), tb.rys_off[N], 2 * N, f, k, s);
+}
+
+// 2D Rys integrals of one (root, axis): VRR to V[e][f] (e <= LA+LB,
+// f <= LC+LD) from
+//   V[e+1][f] = C00 V[e][f] + e B10 V[e-1][f] + f B00 V[e][f-1]
+//   V[e][f+1] = C0p V[e][f] + f B01 V[e][f-1] + e B00 V[e-1][f]
+// then both horizontal transfers in closed form:
+//   G[a][b][c][d] = sum_{i<=b} sum_{j<=d} C(b,i) AB^(b-i) C(d,j) CD^(d-j) V[a+i][c+j]
+// (AB = A - B, CD = C - D along the axis).  G layout: ((a*(LB+1)+b)*(LC+1)+c)*(LD+1)+d.
+template <int LA, int LB, int LC, int LD, typename R, typename GPtr>
+__device__ __forceinline__ void build_g(R c00, R c0p, R b10, R b01, R b00, R g00, R ab, R cd,
+                                        GPtr G) {
+  constexpr int LAB = LA + LB, LCD = LC + LD;
+  R v[LAB + 1][LCD + 1];
+  v[0][0] = g00;
+  if (LAB > 0) v[1][0] = c00 * g00;
+#pragma unroll
+  for (int e = 1; e < LAB; ++e) v[e + 1][0] = c00 * v[e][0] + R(e) * b10 * v[e - 1][0];
+#pragma unroll
+  for (int f = 0; f < LCD; ++f) {
+#pragma unroll
+    for (int e = 0; e <= LAB; ++e) {
+      R val = c0p * v[e][f];
+      if (f > 0) val += R(f) * b01 * v[e][f - 1];
+      if (e > 0) val += R(e) * b00 * v[e - 1][f];
+      v[e][f + 1] = val;
+    }
+  }
+  R abp[LB + 1], cdp[LD + 1];
+  abp[0] = R(1);
+#pragma unroll
+  for (int i = 1; i <= LB; ++i) abp[i] = abp[i - 1] * ab;
+  cdp[0] = R(1);
+#pragma unroll
+  for (int i = 1; i <= LD; ++i) cdp[i] = cdp[i - 1] * cd;
+#pragma unroll
+  for (int a = 0; a <= LA; ++a)
+#pragma unroll
+    for (int b = 0; b <= LB; ++b)
+#pragma unroll
+      for (int c = 0; c <= LC; ++c)
+#pragma unroll
+        for (int d = 0; d <= LD; ++d) {
+          R acc = R(0);
+#pragma unroll
+          for (int i = 0; i <= b; ++i)
+#pragma unroll
+            for (int j = 0; j <= d; ++j)
+              acc += R(binom(b, i) * binom(d, j)) * abp[b - i] * cdp[d - j] * v[a + i][c + j];
+          G[((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d] = acc;
+        }
+}
+
+}  // namespace b200jk

@@ -1,0 +1,93 @@
+// Launcher table filled by the per-bra-class translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace b200jk {
+
+struct JKArgs;
+struct GradArgs;
+
+constexpr int kMaxL = 3;
+constexpr int kPairClasses = (kMaxL + 1) * (kMaxL + 2) / 2;              // 10
+constexpr int kQuartetClasses = kPairClasses * (kPairClasses + 1) / 2;   // 55
+
+using JKLauncher = int (*)(const JKArgs&, cudaStream_t);
+using SchwarzLauncher = int (*)(const JKArgs&, int npairs, int cart, cudaStream_t);
+using GradLauncher = int (*)(const GradArgs&, cudaStream_t);
+
+struct DispatchTable {
+  JKLauncher jk64[kQuartetClasses] = {};
+  JKLauncher jk32[kQuartetClasses] = {};
+  GradLauncher grad64[kQuartetClasses] = {};
+  SchwarzLauncher schwarz[kPairClasses] = {};
+  bool reg_path[kQuartetClasses] = {};
+  int team[kQuartetClasses] = {};
+};
+
+inline int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }   // la >= lb
+inline int quartet_class(int x, int y) { return x * (x + 1) / 2 + y; }      // x >= y
+
+#define B200JK_FOR_EACH_CLASS_PAIR(M) \
+  M(0, 0) \
+  M(1, 0) \
+  M(1, 1) \
+  M(2, 0) \
+  M(2, 1) \
+  M(2, 2) \
+  M(3, 0) \
+  M(3, 1) \
+  M(3, 2) \
+  M(3, 3) \
+  M(4, 0) \
+  M(4, 1) \
+  M(4, 2) \
+  M(4, 3) \
+  M(4, 4) \
+  M(5, 0) \
+  M(5, 1) \
+  M(5, 2) \
+  M(5, 3) \
+  M(5, 4) \
+  M(5, 5) \
+  M(6, 0) \
+  M(6, 1) \
+  M(6, 2) \
+  M(6, 3) \
+  M(6, 4) \
+  M(6, 5) \
+  M(6, 6) \
+  M(7, 0) \
+  M(7, 1) \
+  M(7, 2) \
+  M(7, 3) \
+  M(7, 4) \
+  M(7, 5) \
+  M(7, 6) \
+  M(7, 7) \
+  M(8, 0) \
+  M(8, 1) \
+  M(8, 2) \
+  M(8, 3) \
+  M(8, 4) \
+  M(8, 5) \
+  M(8, 6) \
+  M(8, 7) \
+  M(8, 8) \
+  M(9, 0) \
+  M(9, 1) \
+  M(9, 2) \
+  M(9, 3) \
+  M(9, 4) \
+  M(9, 5) \
+  M(9, 6) \
+  M(9, 7) \
+  M(9, 8) \
+  M(9, 9)
+#define B200JK_DECLARE_REG(x, y) void register_jk_class_##x##_##y(DispatchTable&);
+B200JK_FOR_EACH_CLASS_PAIR(B200JK_DECLARE_REG)
+#undef B200JK_DECLARE_REG
+void register_grad_classes(DispatchTable&);
+
+const DispatchTable& dispatch();
+
+}  // namespace b200jk

@@ -1,0 +1,808 @@
+// Plan construction, basis transforms, J/K orchestration and the C ABI.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/b200jk.h"
+#include "jk_kernels.cuh"
+#include "plan.h"
+#include "rys_tables.h"
+
+namespace b200jk {
+
+// ---------------------------------------------------------------- errors
+static thread_local std::string g_error;
+void set_error(const std::string& msg) { g_error = msg; }
+
+struct Failure {
+  int code;
+  std::string msg;
+};
+
+#define CUDA_OK(expr)                                                                   \
+  do {                                                                                  \
+    cudaError_t _e = (expr);                                                            \
+    if (_e != cudaSuccess)                                                              \
+      throw Failure{B200JK_INTERNAL, std::string(#expr) + ": " + cudaGetErrorString(_e)}; \
+  } while (0)
+
+static void invalid(const std::string& m) { throw Failure{B200JK_INVALID_ARGUMENT, m}; }
+
+// ---------------------------------------------------------------- dispatch
+const DispatchTable& dispatch() {
+  static DispatchTable table;
+  static std::once_flag once;
+  std::call_once(once, [] {
+#define B200JK_CALL_REG(x, y) register_jk_class_##x##_##y(table);
+    B200JK_FOR_EACH_CLASS_PAIR(B200JK_CALL_REG)
+#undef B200JK_CALL_REG
+    register_grad_classes(table);
+  });
+  return table;
+}
+
+// ---------------------------------------------------------------- transforms
+// Output transform of shell l: column f of row c is the coefficient of raw
+// Cartesian component c (x^lx y^ly z^lz times the normalised radial part) in
+// output function f.  Spherical: real solid harmonics r^l Y_lm, m = -l..l
+// (p: x, y, z), with the closed form of Helgaker, Jorgensen & Olsen,
+// "Molecular Electronic-Structure Theory" eq. 6.4.47-6.4.50, times
+// sqrt((2l+1)/4pi).  Cartesian: libcint keeps the angular factors
+// 1/(2 sqrt(pi)) and sqrt(3/(4 pi)) on s and p functions and none above.
+static double fact(int n) { double r = 1; for (int i = 2; i <= n; ++i) r *= i; return r; }
+static double binomd(int n, int k) { return (k < 0 || k > n) ? 0.0 : fact(n) / (fact(k) * fact(n - k)); }
+
+static void output_transform(int l, int cart, double* t /* [10][10] */) {
+  std::fill(t, t + kTS, 0.0);
+  const int nc = (l + 1) * (l + 2) / 2;
+  if (cart) {
+    const double f = l == 0 ? 0.282094791773878143 : (l == 1 ? 0.488602511902919921 : 1.0);
+    for (int c = 0; c < nc; ++c) t[c * kTW + c] = f;
+    return;
+  }
+  const double norm = std::sqrt((2 * l + 1) / (4 * M_PI));
+  for (int m = -l; m <= l; ++m) {
+    const int am = std::abs(m);
+    int col = m + l;
+    if (l == 1) col = m == 1 ? 0 : (m == -1 ? 1 : 2);
+    const double nlm = 1.0 / (std::pow(2.0, am) * fact(l)) *
+                       std::sqrt(2.0 * fact(l + am) * fact(l - am) / (m == 0 ? 2.0 : 1.0));
+    for (int tt = 0; tt <= (l - am) / 2; ++tt)
+      for (int u = 0; u <= tt; ++u)
+        for (int v2 = (m < 0 ? 1 : 0); v2 <= am; v2 += 2) {
+          const int sgn_exp = tt + (v2 - (m < 0 ? 1 : 0)) / 2;
+          const double coef = (sgn_exp % 2 ? -1.0 : 1.0) * std::pow(0.25, tt) * binomd(l, tt) *
+                              binomd(l - tt, am + tt) * binomd(tt, u) * binomd(am, v2);
+          const int px = 2 * tt + am - 2 * u - v2, py = 2 * u + v2, pz = l - 2 * tt - am;
+          const int c = (l - px) * (l - px + 1) / 2 + pz;
+          (void)py;
+          t[c * kTW + col] += norm * nlm * coef;
+        }
+  }
+}
+
+// ---------------------------------------------------------------- tables
+struct DeviceTables {
+  Tables t{};
+  DevBuf rys, rys_f, off, nint, ar, aw, boys, boys_f, c2s_sph, c2s_cart;
+  Tables sph, cartt;
+};
+
+static std::mutex g_tables_mu;
+static std::map<int, DeviceTables*> g_tables;
+
+static DeviceTables& tables_for(int device) {
+  std::lock_guard<std::mutex> lock(g_tables_mu);
+  auto it = g_tables.find(device);
+  if (it != g_tables.end()) return *it->second;
+  auto* d = new DeviceTables();
+  auto up = [](DevBuf& b, const void* src, size_t n) {
+    CUDA_OK(b.ensure(n));
+    CUDA_OK(cudaMemcpy(b.ptr, src, n, cudaMemcpyHostToDevice));
+  };
+  up(d->rys, kRysTable, sizeof(kRysTable));
+  std::vector<float> rf(kRysTable, kRysTable + RYS_TABLE_SIZE);
+  up(d->rys_f, rf.data(), rf.size() * sizeof(float));
+  up(d->off, kRysOffset, sizeof(kRysOffset));
+  up(d->nint, kRysIntervals, sizeof(kRysIntervals));
+  up(d->ar, kRysAsymR, sizeof(kRysAsymR));
+  up(d->aw, kRysAsymW, sizeof(kRysAsymW));
+  up(d->boys, kBoysGrid, sizeof(kBoysGrid));
+  std::vector<float> bf(kBoysGrid, kBoysGrid + BOYS_NROW * BOYS_NCOL);
+  up(d->boys_f, bf.data(), bf.size() * sizeof(float));
+  std::vector<double> cs(4 * kTS), cc(4 * kTS);
+  for (int l = 0; l <= 3; ++l) {
+    output_transform(l, 0, cs.data() + l * kTS);
+    output_transform(l, 1, cc.data() + l * kTS);
+  }
+  up(d->c2s_sph, cs.data(), cs.size() * sizeof(double));
+  up(d->c2s_cart, cc.data(), cc.size() * sizeof(double));
+  Tables base{};
+  base.rys = d->rys.as<double>();
+  base.rys_f = d->rys_f.as<float>();
+  base.rys_off = d->off.as<int>();
+  base.rys_nint = d->nint.as<int>();
+  base.asym_r = d->ar.as<double>();
+  base.asym_w = d->aw.as<double>();
+  base.boys = d->boys.as<double>();
+  base.boys_f = d->boys_f.as<float>();
+  d->sph = base;
+  d->sph.c2s = d->c2s_sph.as<double>();
+  d->cartt = base;
+  d->cartt.c2s = d->c2s_cart.as<double>();
+  g_tables[device] = d;
+  return *d;
+}
+
+static Tables plan_tables(const Plan& p) {
+  DeviceTables& d = tables_for(p.device);
+  return p.cart ? d.cartt : d.sph;
+}
+
+// ---------------------------------------------------------------- small kernels
+// Input densities (output basis, packed per molecule) -> raw Cartesian
+// effective densities: symmetric part (all nb) then, if hermi == 0, the
+// antisymmetric part.  Also flags a nonfinite density in *status.
+__global__ void density_in_kernel(const double* __restrict__ din, int nb, int hermi,
+                                  double* __restrict__ dout, long long out_stride,
+                                  long long cart_stride, const long long* mol_out_base,
+                                  const int* mol_nout, const long long* mol_cart_base,
+                                  const int* mol_ncart, const int* cart_ws, const int4* ws_info,
+                                  const int* mol_cart_ao, const double* c2s, int* status) {
+  const int mol = blockIdx.y;
+  const int e = blockIdx.z;
+  const int nc = mol_ncart[mol];
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)nc * nc) return;
+  const int i = (int)(idx / nc), j = (int)(idx % nc);
+  const int no = mol_nout[mol];
+  const int wi = cart_ws[mol_cart_ao[mol] + i], wj = cart_ws[mol_cart_ao[mol] + j];
+  const int4 si = ws_info[wi], sj = ws_info[wj];
+  const int ci = i - si.x, cj = j - sj.x;
+  const double* ti = c2s + si.y * kTS + ci * kTW;
+  const double* tj = c2s + sj.y * kTS + cj * kTW;
+  const double* d = din + (long long)e * out_stride + mol_out_base[mol];
+  double sym = 0.0, anti = 0.0;
+  bool finite = true;
+  for (int fa = 0; fa < kTW; ++fa) {
+    const double x = ti[fa];
+    if (x == 0.0) continue;
+    for (int fb = 0; fb < kTW; ++fb) {
+      const double y = tj[fb];
+      if (y == 0.0) continue;
+      const double dab = d[(long long)(si.w + fa) * no + sj.w + fb];
+      const double dba = d[(long long)(sj.w + fb) * no + si.w + fa];
+      finite = finite && isfinite(dab);
+      sym += x * y * (dab + dba);
+      anti += x * y * (dab - dba);
+    }
+  }
+  if (!finite) atomicOr(status, 1);
+  const long long o = mol_cart_base[mol] + (long long)i * nc + j;
+  dout[(long long)e * cart_stride + o] = 0.5 * sym;
+  if (!hermi) dout[(long long)(nb + e) * cart_stride + o] = 0.5 * anti;
+}
+
+// MJ/MK (raw Cartesian, unsymmetrised) -> J/K in the output basis.
+__global__ void jk_out_kernel(const double* __restrict__ vj, const double* __restrict__ vk, int nb,
+                              int hermi, int with_j, int with_k, double* __restrict__ out,
+                              long long out_stride, long long cart_stride,
+                              const long long* mol_out_base, const int* mol_nout,
+                              const long long* mol_cart_base, const int* mol_ncart,
+                              const int* out_ws, const int4* ws_info, const int* mol_out_ao,
+                              const double* c2s) {
+  const int mol = blockIdx.y;
+  const int e = blockIdx.z;
+  const int no = mol_nout[mol];
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)no * no) return;
+  const int a = (int)(idx / no), b = (int)(idx % no);
+  const int wa = out_ws[mol_out_ao[mol] + a], wb = out_ws[mol_out_ao[mol] + b];
+  const int4 sa = ws_info[wa], sb = ws_info[wb];
+  const int fa = a - sa.w, fb = b - sb.w;
+  const int na = (sa.y + 1) * (sa.y + 2) / 2, nbf = (sb.y + 1) * (sb.y + 2) / 2;
+  const double* ta = c2s + sa.y * kTS;
+  const double* tb = c2s + sb.y * kTS;
+  const int nc = mol_ncart[mol];
+  const long long cb = mol_cart_base[mol];
+  double jv = 0.0, kv = 0.0;
+  for (int i = 0; i < na; ++i) {
+    const double x = ta[i * kTW + fa];
+    if (x == 0.0) continue;
+    const int ci = sa.x + i;
+    for (int j = 0; j < nbf; ++j) {
+      const double y = tb[j * kTW + fb];
+      if (y == 0.0) continue;
+      const int cj = sb.x + j;
+      const long long ij = cb + (long long)ci * nc + cj, ji = cb + (long long)cj * nc + ci;
+      if (with_j) {
+        const double* m = vj + (long long)e * cart_stride;
+        jv += x * y * (m[ij] + m[ji]);
+      }
+      if (with_k) {
+        const double* m = vk + (long long)e * cart_stride;
+        double v = m[ij] + m[ji];
+        if (!hermi) {
+          const double* ma = vk + (long long)(nb + e) * cart_stride;
+          v += ma[ij] - ma[ji];
+        }
+        kv += x * y * v;
+      }
+    }
+  }
+  const long long o = mol_out_base[mol] + (long long)a * no + b;
+  if (with_j) out[(long long)e * out_stride + o] = jv;
+  if (with_k) out[(long long)((with_j ? nb : 0) + e) * out_stride + o] = kv;
+}
+
+__global__ void maxabs_kernel(const double* __restrict__ x, long long n, double* out) {
+  double m = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double v = fabs(x[i]);
+    if (v > m) m = v;
+  }
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0 && m > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long*>(out), (unsigned long long)__double_as_longlong(m));
+}
+
+// First ket position (within the bra's ket range) computed in FP32:
+// Q_bra * Q_ket * max|D| < fp32_cut.  Ket bounds are sorted descending.
+__global__ void split_kernel(const int2* __restrict__ bra_kets, const double* __restrict__ bra_q,
+                             const double* __restrict__ ket_q, const double* maxd, double fp32_cut,
+                             int nbra, int* __restrict__ split) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbra) return;
+  const int2 r = bra_kets[b];
+  const double f = bra_q[b] * (*maxd);
+  int lo = r.x, hi = r.y;
+  // invariant: kets < lo are FP64, kets >= hi are FP32
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ket_q[mid] * f < fp32_cut) hi = mid;
+    else lo = mid + 1;
+  }
+  split[b] = lo;
+}
+
+// ---------------------------------------------------------------- plan creation
+static int ncart_of(int l) { return (l + 1) * (l + 2) / 2; }
+
+struct PrimPair {
+  double4 data;
+  double k;
+};
+
+static void validate_tables(const b200jk_molecule& m, int cart) {
+  // csrc/tables.h:40-75
+  if (m.natm < 0 || m.nbas < 1 || m.nenv < 20 || (cart != 0 && cart != 1) || !m.atm || !m.bas || !m.env)
+    invalid("Invalid libcint table dimensions or operator");
+  for (int i = 0; i < m.nenv; ++i)
+    if (!std::isfinite(m.env[i])) invalid("Native integral env must be finite");
+  if (m.env[8] != 0.0) throw Failure{B200JK_UNSUPPORTED, "Range-separated (omega != 0) J/K is not built on the B200 path"};
+  for (int a = 0; a < m.natm; ++a) {
+    const int32_t* row = m.atm + a * 6;
+    if (row[1] < 20 || row[1] + 3 > m.nenv || row[2] != 1)
+      invalid("Native backend requires valid point nuclei");
+  }
+  for (int s = 0; s < m.nbas; ++s) {
+    const int32_t* row = m.bas + s * 8;
+    const int l = row[1], np = row[2], nc = row[3];
+    if (row[0] < 0 || row[0] >= m.natm || l < 0 || l > 12 || np < 1 || np > 64 || nc < 1 || nc > 64 ||
+        row[4] != 0 || row[5] < 20 || row[5] + np > m.nenv || row[6] < 20 ||
+        (long long)row[6] + (long long)np * nc > m.nenv)
+      invalid("Invalid or unsupported libcint basis table");
+    for (int p = 0; p < np; ++p)
+      if (m.env[row[5] + p] <= 0.0) invalid("Gaussian exponents must be positive");
+    if (l > kMaxL)
+      throw Failure{B200JK_UNSUPPORTED, "Angular momentum above f (l > 3) is not built on the B200 path"};
+  }
+}
+
+static void upload(DevBuf& b, const void* src, size_t n) {
+  CUDA_OK(b.ensure(n));
+  if (n) CUDA_OK(cudaMemcpy(b.ptr, src, n, cudaMemcpyHostToDevice));
+}
+
+static JKArgs base_args(const Plan& p) {
+  JKArgs a{};
+  a.sh_info = p.d_ws_info.as<int4>();
+  a.sh_xyz = p.d_ws_xyz.as<double4>();
+  a.pair_info = p.d_pair_info.as<int4>();
+  a.pp_data = p.d_pp_data.as<double4>();
+  a.pp_k = p.d_pp_k.as<double>();
+  a.mol_base = p.d_mol_base_cart.as<long long>();
+  a.mol_n = p.d_mol_ncart.as<int>();
+  a.tb = plan_tables(p);
+  a.status = p.d_status.as<int>();
+  return a;
+}
+
+static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double cut, int device) {
+  if (nmol < 1 || !mols) invalid("At least one molecule is required");
+  if (!std::isfinite(cut) || cut < 0) invalid("Invalid Schwarz cutoff");
+  if (cart != 0 && cart != 1) invalid("cart must be 0 or 1");
+  for (int m = 0; m < nmol; ++m) validate_tables(mols[m], cart);
+  CUDA_OK(cudaSetDevice(device));
+  auto plan = std::make_unique<Plan>();
+  Plan& p = *plan;
+  p.device = device;
+  p.cart = cart;
+  p.cutoff = cut;
+  p.nmol = nmol;
+  // ---- work shells (one per contraction column of every shell)
+  std::vector<int> parent_base(nmol + 1, 0);
+  int atm_base = 0;
+  for (int m = 0; m < nmol; ++m) {
+    const auto& M = mols[m];
+    parent_base[m + 1] = parent_base[m] + M.nbas;
+    int out = 0, cartn = 0;
+    p.mol_atm_off.push_back(atm_base);
+    for (int a = 0; a < M.natm; ++a) {
+      const double* r = M.env + M.atm[a * 6 + 1];
+      p.atom_xyzq.push_back(make_double4(r[0], r[1], r[2], (double)M.atm[a * 6 + 0]));
+    }
+    for (int s = 0; s < M.nbas; ++s) {
+      const int32_t* row = M.bas + s * 8;
+      const int l = row[1], np = row[2], nc = row[3];
+      const double* r = M.env + M.atm[row[0] * 6 + 1];
+      const int nf = cart ? ncart_of(l) : 2 * l + 1;
+      for (int c = 0; c < nc; ++c) {
+        p.ws_info.push_back(make_int4(cartn, l, m, out + c * nf));
+        p.ws_xyz.push_back(make_double4(r[0], r[1], r[2], 0.0));
+        p.ws_parent.push_back(parent_base[m] + s);
+        p.ws_atm.push_back(atm_base + row[0]);
+        p.ws_nprim.push_back(np);
+        p.ws_prim_off.push_back((int)p.ws_exp.size());
+        for (int q = 0; q < np; ++q) {
+          p.ws_exp.push_back(M.env[row[5] + q]);
+          p.ws_coef.push_back(M.env[row[6] + c * np + q]);
+        }
+        cartn += ncart_of(l);
+      }
+      out += nc * nf;
+    }
+    p.mol_nout.push_back(out);
+    p.mol_ncart.push_back(cartn);
+    p.mol_natm.push_back(M.natm);
+    atm_base += M.natm;
+  }
+  p.total_atm = atm_base;
+  p.nws = (int)p.ws_info.size();
+  long long ob = 0, cb = 0;
+  for (int m = 0; m < nmol; ++m) {
+    p.mol_out_base.push_back(ob);
+    p.mol_cart_base.push_back(cb);
+    ob += (long long)p.mol_nout[m] * p.mol_nout[m];
+    cb += (long long)p.mol_ncart[m] * p.mol_ncart[m];
+  }
+  p.out_stride = ob;
+  p.cart_stride = cb;
+  // ---- shell pairs and primitive pairs
+  std::vector<double4> pp_data;
+  std::vector<double> pp_k;
+  int ws0 = 0;
+  for (int m = 0; m < nmol; ++m) {
+    int wsn = ws0;
+    while (wsn < p.nws && p.ws_info[wsn].z == m) ++wsn;
+    for (int i = ws0; i < wsn; ++i)
+      for (int j = ws0; j <= i; ++j) {
+        int A = i, B = j;
+        if (p.ws_info[B].y > p.ws_info[A].y) std::swap(A, B);
+        const double4 ra = p.ws_xyz[A], rb = p.ws_xyz[B];
+        const double ab2 = (ra.x - rb.x) * (ra.x - rb.x) + (ra.y - rb.y) * (ra.y - rb.y) +
+                           (ra.z - rb.z) * (ra.z - rb.z);
+        const int off = (int)pp_data.size();
+        for (int ia = 0; ia < p.ws_nprim[A]; ++ia)
+          for (int ib = 0; ib < p.ws_nprim[B]; ++ib) {
+            const double a = p.ws_exp[p.ws_prim_off[A] + ia], b = p.ws_exp[p.ws_prim_off[B] + ib];
+            const double ca = p.ws_coef[p.ws_prim_off[A] + ia], cbv = p.ws_coef[p.ws_prim_off[B] + ib];
+            const double pe = a + b;
+            const double expo = a * b / pe * ab2;
+            if (expo > 40.0 || ca == 0.0 || cbv == 0.0) continue;  // exp(-40) ~ 4e-18
+            pp_data.push_back(make_double4((a * ra.x + b * rb.x) / pe, (a * ra.y + b * rb.y) / pe,
+                                           (a * ra.z + b * rb.z) / pe, pe));
+            pp_k.push_back(std::exp(-expo) * ca * cbv);
+          }
+        const int cnt = (int)pp_data.size() - off;
+        if (cnt == 0) continue;
+        p.pair_info.push_back(make_int4(A, B, off, cnt));
+        p.pair_class.push_back(pair_class(p.ws_info[A].y, p.ws_info[B].y));
+      }
+    ws0 = wsn;
+  }
+  p.npair = (int)p.pair_info.size();
+  // ---- device upload
+  upload(p.d_ws_info, p.ws_info.data(), p.ws_info.size() * sizeof(int4));
+  upload(p.d_ws_xyz, p.ws_xyz.data(), p.ws_xyz.size() * sizeof(double4));
+  upload(p.d_pair_info, p.pair_info.data(), p.pair_info.size() * sizeof(int4));
+  upload(p.d_pp_data, pp_data.data(), pp_data.size() * sizeof(double4));
+  upload(p.d_pp_k, pp_k.data(), pp_k.size() * sizeof(double));
+  upload(p.d_mol_base_cart, p.mol_cart_base.data(), nmol * sizeof(long long));
+  upload(p.d_mol_ncart, p.mol_ncart.data(), nmol * sizeof(int));
+  upload(p.d_mol_base_out, p.mol_out_base.data(), nmol * sizeof(long long));
+  upload(p.d_mol_nout, p.mol_nout.data(), nmol * sizeof(int));
+  {
+    std::vector<int> cart_ws, out_ws;
+    for (int w = 0; w < p.nws; ++w) {
+      const int l = p.ws_info[w].y;
+      for (int c = 0; c < ncart_of(l); ++c) cart_ws.push_back(w);
+      for (int c = 0; c < (cart ? ncart_of(l) : 2 * l + 1); ++c) out_ws.push_back(w);
+    }
+    upload(p.d_cart_ws, cart_ws.data(), cart_ws.size() * sizeof(int));
+    upload(p.d_out_ws, out_ws.data(), out_ws.size() * sizeof(int));
+  }
+  upload(p.d_atoms, p.atom_xyzq.data(), p.atom_xyzq.size() * sizeof(double4));
+  upload(p.d_ws_atm, p.ws_atm.data(), p.ws_atm.size() * sizeof(int));
+  {
+    std::vector<double2> ec(p.ws_exp.size());
+    for (size_t i = 0; i < ec.size(); ++i) ec[i] = make_double2(p.ws_exp[i], p.ws_coef[i]);
+    upload(p.d_ws_prim, ec.data(), ec.size() * sizeof(double2));
+    upload(p.d_ws_prim_off, p.ws_prim_off.data(), p.ws_prim_off.size() * sizeof(int));
+  }
+  CUDA_OK(p.d_status.ensure(sizeof(int)));
+  CUDA_OK(cudaMemset(p.d_status.ptr, 0, sizeof(int)));
+  CUDA_OK(p.d_maxd.ensure(sizeof(double)));
+  // ---- Schwarz bounds on the device, one launch per pair class
+  std::vector<std::vector<int>> by_class(kPairClasses);
+  for (int q = 0; q < p.npair; ++q) by_class[p.pair_class[q]].push_back(q);
+  CUDA_OK(p.d_q_work.ensure(std::max(p.npair, 1) * sizeof(double)));
+  {
+    std::vector<DevBuf> lists(kPairClasses);
+    for (int c = 0; c < kPairClasses; ++c) {
+      if (by_class[c].empty()) continue;
+      upload(lists[c], by_class[c].data(), by_class[c].size() * sizeof(int));
+      JKArgs a = base_args(p);
+      a.bra_pairs = lists[c].as<int>();
+      a.q_out = p.d_q_work.as<double>();
+      const int rc = dispatch().schwarz[c](a, (int)by_class[c].size(), cart, 0);
+      if (rc) throw Failure{B200JK_INTERNAL, std::string("Schwarz launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+    }
+    CUDA_OK(cudaDeviceSynchronize());
+  }
+  std::vector<double> qw(p.npair);
+  if (p.npair) CUDA_OK(cudaMemcpy(qw.data(), p.d_q_work.ptr, p.npair * sizeof(double), cudaMemcpyDeviceToHost));
+  // parent-pair bound: max over the work pairs of the parent pair
+  std::map<std::pair<int, int>, double> parent;
+  auto pkey = [&](int q) {
+    int a = p.ws_parent[p.pair_info[q].x], b = p.ws_parent[p.pair_info[q].y];
+    if (a < b) std::swap(a, b);
+    return std::make_pair(a, b);
+  };
+  for (int q = 0; q < p.npair; ++q) {
+    auto k = pkey(q);
+    auto it = parent.find(k);
+    if (it == parent.end()) parent[k] = qw[q];
+    else it->second = std::max(it->second, qw[q]);
+  }
+  p.pair_q.resize(p.npair);
+  std::vector<double> qmax_mol(nmol, 0.0);
+  for (int q = 0; q < p.npair; ++q) {
+    p.pair_q[q] = std::sqrt(parent[pkey(q)]);
+    const int m = p.ws_info[p.pair_info[q].x].z;
+    qmax_mol[m] = std::max(qmax_mol[m], p.pair_q[q]);
+  }
+  // ---- class lists: significant pairs sorted by (molecule, Q desc, id)
+  for (int c = 0; c < kPairClasses; ++c) {
+    ClassList& L = p.classes[c];
+    std::vector<int> ids;
+    for (int q : by_class[c]) {
+      const int m = p.ws_info[p.pair_info[q].x].z;
+      if (cut > 0 && p.pair_q[q] * qmax_mol[m] < cut) continue;  // coulomb_shells.h:203
+      ids.push_back(q);
+    }
+    std::sort(ids.begin(), ids.end(), [&](int a, int b) {
+      const int ma = p.ws_info[p.pair_info[a].x].z, mb = p.ws_info[p.pair_info[b].x].z;
+      if (ma != mb) return ma < mb;
+      if (p.pair_q[a] != p.pair_q[b]) return p.pair_q[a] > p.pair_q[b];
+      return a < b;
+    });
+    L.pairs = ids;
+    L.q.resize(ids.size());
+    for (size_t i = 0; i < ids.size(); ++i) L.q[i] = p.pair_q[ids[i]];
+    L.mol_begin.assign(nmol + 1, 0);
+    for (int q : ids) L.mol_begin[p.ws_info[p.pair_info[q].x].z + 1]++;
+    for (int m = 0; m < nmol; ++m) L.mol_begin[m + 1] += L.mol_begin[m];
+    upload(L.d_pairs, ids.data(), ids.size() * sizeof(int));
+    upload(L.d_q, L.q.data(), L.q.size() * sizeof(double));
+  }
+  // ---- work items per class pair (X >= Y)
+  const auto& disp = dispatch();
+  for (int x = 0; x < kPairClasses; ++x)
+    for (int y = 0; y <= x; ++y) {
+      const ClassList& X = p.classes[x];
+      const ClassList& Y = p.classes[y];
+      if (X.pairs.empty() || Y.pairs.empty()) continue;
+      const int cls = quartet_class(x, y);
+      const int chunk = disp.reg_path[cls] ? 256 : std::max(8, 4 * (128 / disp.team[cls]));
+      auto* W = new ClassPairWork();
+      W->x = x;
+      W->y = y;
+      W->nbra = (int)X.pairs.size();
+      std::vector<int4> items;
+      std::vector<int2> bk(W->nbra);
+      for (int bp = 0; bp < W->nbra; ++bp) {
+        const int m = p.ws_info[p.pair_info[X.pairs[bp]].x].z;
+        const int lo = Y.mol_begin[m], hi0 = Y.mol_begin[m + 1];
+        int hi = hi0;
+        if (cut > 0) {
+          const double qb = X.q[bp];
+          int a = lo, b = hi0;  // first ket with qb*qk < cut
+          while (a < b) {
+            const int mid = (a + b) >> 1;
+            if (qb * Y.q[mid] < cut) b = mid;
+            else a = mid + 1;
+          }
+          hi = a;
+        }
+        if (x == y) hi = std::min(hi, bp + 1);
+        if (hi < lo) hi = lo;
+        bk[bp] = make_int2(lo, hi);
+        W->quartets += hi - lo;
+        for (int s = lo; s < hi; s += chunk) items.push_back(make_int4(bp, s, std::min(hi, s + chunk), 0));
+      }
+      W->nwork = (int)items.size();
+      if (W->nwork == 0) { delete W; continue; }
+      upload(W->work, items.data(), items.size() * sizeof(int4));
+      upload(W->bra_kets, bk.data(), bk.size() * sizeof(int2));
+      CUDA_OK(W->split.ensure(W->nbra * sizeof(int)));
+      p.work.push_back(W);
+    }
+  // ---- quartet count on the reference's shells (parent pairs, canonical)
+  {
+    long long total = 0;
+    std::vector<std::vector<double>> pq(nmol);
+    // parent pair bounds per molecule
+    std::map<std::pair<int, int>, double> seen;
+    for (int q = 0; q < p.npair; ++q) seen[pkey(q)] = p.pair_q[q];
+    for (auto& kv : seen) {
+      int m = 0;
+      while (m + 1 < nmol + 1 && parent_base[m + 1] <= kv.first.first) ++m;
+      pq[m].push_back(kv.second);
+    }
+    for (int m = 0; m < nmol; ++m) {
+      auto& v = pq[m];
+      std::sort(v.begin(), v.end(), std::greater<double>());
+      for (size_t a = 0; a < v.size(); ++a) {
+        if (cut <= 0) { total += (long long)a + 1; continue; }
+        // count b <= a (in sorted order) with v[a]*v[b] >= cut: all b < a have v[b] >= v[a]
+        size_t lo = 0, hi = a + 1;
+        while (lo < hi) {
+          const size_t mid = (lo + hi) / 2;
+          if (v[a] * v[mid] < cut) hi = mid;
+          else lo = mid + 1;
+        }
+        total += (long long)lo;
+      }
+    }
+    p.quartets = total;
+  }
+  return plan.release();
+}
+
+// ---------------------------------------------------------------- J/K execution
+static void ensure_scratch(Plan& p, int nb) {
+  if (p.scratch_nb >= nb) return;
+  CUDA_OK(p.d_dens.ensure((size_t)2 * nb * p.cart_stride * sizeof(double)));
+  CUDA_OK(p.d_vj.ensure((size_t)nb * p.cart_stride * sizeof(double)));
+  CUDA_OK(p.d_vk.ensure((size_t)2 * nb * p.cart_stride * sizeof(double)));
+  p.scratch_nb = nb;
+}
+
+static int max_nc(const Plan& p) { return *std::max_element(p.mol_ncart.begin(), p.mol_ncart.end()); }
+static int max_no(const Plan& p) { return *std::max_element(p.mol_nout.begin(), p.mol_nout.end()); }
+
+static void run_jk(Plan& p, const double* d_in, int nb, double* d_out, int with_j, int with_k,
+                   int hermi, int precision, double fp32_cut, cudaStream_t st) {
+  if (nb < 1) invalid("Direct J/K requires at least one density");
+  if ((with_j != 0 && with_j != 1) || (with_k != 0 && with_k != 1) || !(with_j || with_k))
+    invalid("Direct J/K requires at least one selected operator");
+  if (precision != B200JK_FP64 && precision != B200JK_SPLIT) invalid("Unknown precision mode");
+  if (precision == B200JK_SPLIT && !(fp32_cut >= 0 && std::isfinite(fp32_cut))) invalid("Invalid fp32_cut");
+  if (!d_in || !d_out) invalid("Null density or output pointer");
+  CUDA_OK(cudaSetDevice(p.device));
+  ensure_scratch(p, nb);
+  const int ndm = hermi ? nb : 2 * nb;
+  const Tables tb = plan_tables(p);
+  // molecule AO starts (global cart / out AO index)
+  if (!p.d_mol_ao_off.ptr) {
+    std::vector<int> v(2 * p.nmol);
+    int c = 0, o = 0;
+    for (int m = 0; m < p.nmol; ++m) {
+      v[m] = c;
+      v[p.nmol + m] = o;
+      c += p.mol_ncart[m];
+      o += p.mol_nout[m];
+    }
+    upload(p.d_mol_ao_off, v.data(), v.size() * sizeof(int));
+  }
+  const int* d_mol_cart_ao = p.d_mol_ao_off.as<int>();
+  const int* d_mol_out_ao = d_mol_cart_ao + p.nmol;
+  {
+    const int nc = max_nc(p);
+    const long long n2 = (long long)nc * nc;
+    dim3 grid((unsigned)((n2 + 255) / 256), p.nmol, nb);
+    density_in_kernel<<<grid, 256, 0, st>>>(
+        d_in, nb, hermi, p.d_dens.as<double>(), p.out_stride, p.cart_stride,
+        p.d_mol_base_out.as<long long>(), p.d_mol_nout.as<int>(), p.d_mol_base_cart.as<long long>(),
+        p.d_mol_ncart.as<int>(), p.d_cart_ws.as<int>(), p.d_ws_info.as<int4>(), d_mol_cart_ao, tb.c2s,
+        p.d_status.as<int>());
+    CUDA_OK(cudaGetLastError());
+  }
+  if (with_j) CUDA_OK(cudaMemsetAsync(p.d_vj.ptr, 0, (size_t)nb * p.cart_stride * sizeof(double), st));
+  if (with_k) CUDA_OK(cudaMemsetAsync(p.d_vk.ptr, 0, (size_t)ndm * p.cart_stride * sizeof(double), st));
+  if (precision == B200JK_SPLIT) {
+    CUDA_OK(cudaMemsetAsync(p.d_maxd.ptr, 0, sizeof(double), st));
+    maxabs_kernel<<<592, 256, 0, st>>>(d_in, (long long)nb * p.out_stride, p.d_maxd.as<double>());
+    CUDA_OK(cudaGetLastError());
+    for (auto* W : p.work) {
+      split_kernel<<<(W->nbra + 127) / 128, 128, 0, st>>>(
+          W->bra_kets.as<int2>(), p.classes[W->x].d_q.as<double>(), p.classes[W->y].d_q.as<double>(),
+          p.d_maxd.as<double>(), fp32_cut, W->nbra, W->split.as<int>());
+      CUDA_OK(cudaGetLastError());
+    }
+  }
+  JKArgs a = base_args(p);
+  a.dens = p.d_dens.as<double>();
+  a.vj = p.d_vj.as<double>();
+  a.vk = p.d_vk.as<double>();
+  a.dstride = p.cart_stride;
+  a.ndm = ndm;
+  a.nsym = nb;
+  a.with_j = with_j;
+  a.with_k = with_k;
+  const auto& disp = dispatch();
+  for (auto* W : p.work) {
+    const int cls = quartet_class(W->x, W->y);
+    a.bra_pairs = p.classes[W->x].d_pairs.as<int>();
+    a.ket_pairs = p.classes[W->y].d_pairs.as<int>();
+    a.work = W->work.as<int4>();
+    a.nwork = W->nwork;
+    a.split = W->split.as<int>();
+    if (precision == B200JK_FP64) {
+      a.split_mode = 0;
+      const int rc = disp.jk64[cls](a, st);
+      if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+    } else {
+      a.split_mode = 1;
+      int rc = disp.jk64[cls](a, st);
+      if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+      a.split_mode = 2;
+      rc = disp.jk32[cls](a, st);
+      if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+    }
+  }
+  {
+    const int no = max_no(p);
+    const long long n2 = (long long)no * no;
+    dim3 grid((unsigned)((n2 + 255) / 256), p.nmol, nb);
+    jk_out_kernel<<<grid, 256, 0, st>>>(
+        p.d_vj.as<double>(), p.d_vk.as<double>(), nb, hermi, with_j, with_k, d_out, p.out_stride,
+        p.cart_stride, p.d_mol_base_out.as<long long>(), p.d_mol_nout.as<int>(),
+        p.d_mol_base_cart.as<long long>(), p.d_mol_ncart.as<int>(), p.d_out_ws.as<int>(),
+        p.d_ws_info.as<int4>(), d_mol_out_ao, tb.c2s);
+    CUDA_OK(cudaGetLastError());
+  }
+}
+
+template <typename F>
+static int guarded(F&& f) {
+  try {
+    f();
+    g_error.clear();
+    return B200JK_OK;
+  } catch (const Failure& e) {
+    g_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_error = "host allocation failed";
+    return B200JK_INTERNAL;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return B200JK_INTERNAL;
+  }
+}
+
+}  // namespace b200jk
+
+using namespace b200jk;
+
+struct b200jk_plan {
+  Plan* p;
+};
+
+extern "C" {
+
+const char* b200jk_last_error(void) { return g_error.c_str(); }
+
+int b200jk_plan_create(const b200jk_molecule* mols, int32_t nmol, int32_t cart, double schwarz_cut,
+                       int32_t device, b200jk_plan** out) {
+  return guarded([&] {
+    if (!out) invalid("Null output handle");
+    *out = nullptr;
+    Plan* p = build_plan(mols, nmol, cart, schwarz_cut, device);
+    *out = new b200jk_plan{p};
+  });
+}
+
+void b200jk_plan_destroy(b200jk_plan* plan) {
+  if (!plan) return;
+  cudaSetDevice(plan->p->device);
+  delete plan->p;
+  delete plan;
+}
+
+int b200jk_plan_nao(const b200jk_plan* plan, int32_t mol, int32_t* nao) {
+  return guarded([&] {
+    if (!plan || !nao || mol < 0 || mol >= plan->p->nmol) invalid("Invalid plan query");
+    *nao = plan->p->mol_nout[mol];
+  });
+}
+
+int b200jk_plan_quartets(const b200jk_plan* plan, int64_t* count) {
+  return guarded([&] {
+    if (!plan || !count) invalid("Invalid plan query");
+    *count = plan->p->quartets;
+  });
+}
+
+int b200jk_plan_block_offsets(const b200jk_plan* plan, int64_t* offsets) {
+  return guarded([&] {
+    if (!plan || !offsets) invalid("Invalid plan query");
+    for (int m = 0; m < plan->p->nmol; ++m) offsets[m] = plan->p->mol_out_base[m];
+  });
+}
+
+int b200jk_direct_jk(b200jk_plan* plan, const double* d_density, int32_t nb, double* d_out,
+                     int32_t with_j, int32_t with_k, int32_t hermi, int32_t precision,
+                     double fp32_cut, void* stream) {
+  return guarded([&] {
+    if (!plan) invalid("Null plan");
+    run_jk(*plan->p, d_density, nb, d_out, with_j, with_k, hermi ? 1 : 0, precision, fp32_cut,
+           (cudaStream_t)stream);
+  });
+}
+
+int b200jk_check_status(b200jk_plan* plan, void* stream) {
+  return guarded([&] {
+    if (!plan) invalid("Null plan");
+    Plan& p = *plan->p;
+    CUDA_OK(cudaSetDevice(p.device));
+    CUDA_OK(cudaStreamSynchronize((cudaStream_t)stream));
+    int st = 0;
+    CUDA_OK(cudaMemcpy(&st, p.d_status.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_OK(cudaMemset(p.d_status.ptr, 0, sizeof(int)));
+    if (st & 1) invalid("Nonfinite density");
+    if (st) throw Failure{B200JK_INTERNAL, "device status " + std::to_string(st)};
+  });
+}
+
+int b200jk_direct_jk_tables(const int32_t* atm, int32_t natm, const int32_t* bas, int32_t nbas,
+                            const double* env, int32_t nenv, const double* d_density, int32_t nb,
+                            int32_t n, double* d_out, int32_t cart, double cutoff, int32_t workers,
+                            int32_t with_j, int32_t with_k, void* stream) {
+  return guarded([&] {
+    if (workers < 1) invalid("Direct J/K workers must be positive");
+    int dev = 0;
+    CUDA_OK(cudaGetDevice(&dev));
+    b200jk_molecule m{atm, natm, bas, nbas, env, nenv};
+    std::unique_ptr<Plan> p(build_plan(&m, 1, cart, cutoff, dev));
+    if (n != p->mol_nout[0]) invalid("Direct J/K shape mismatch");
+    run_jk(*p, d_density, nb, d_out, with_j, with_k, 0, B200JK_FP64, 0.0, (cudaStream_t)stream);
+    CUDA_OK(cudaStreamSynchronize((cudaStream_t)stream));
+    int st = 0;
+    CUDA_OK(cudaMemcpy(&st, p->d_status.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st & 1) invalid("Nonfinite density");
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,98 @@
+// Instantiates the J/K kernels of one class pair (BRA_CLASS >= KET_CLASS,
+// compiled once per pair so the classes build in parallel) and registers
+// their launchers in the dispatch table.
+#include "dispatch.h"
+#include "jk_kernels.cuh"
+
+#if !defined(BRA_CLASS) || !defined(KET_CLASS)
+#error "compile with -DBRA_CLASS=<0..9> -DKET_CLASS=<0..BRA_CLASS>"
+#endif
+
+namespace b200jk {
+
+namespace {
+
+constexpr int pc_la(int pc) { return pc == 0 ? 0 : pc <= 2 ? 1 : pc <= 5 ? 2 : 3; }
+constexpr int pc_lb(int pc) { return pc - pc_la(pc) * (pc_la(pc) + 1) / 2; }
+
+// Kernel shape policy: a register path for blocks that fit one thread,
+// otherwise a team whose lanes hold about 24 outputs each.
+template <int LA, int LB, int LC, int LD>
+struct Policy {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  static constexpr bool REG = (3 * CI::NG + CI::NOUT <= 96) && CI::NROOT <= 3;
+  static constexpr int TEAM = CI::NOUT <= 4 * 24 ? 4 : CI::NOUT <= 8 * 24 ? 8 : CI::NOUT <= 16 * 24 ? 16 : 32;
+};
+
+template <int LA, int LB, int LC, int LD, typename R>
+int launch_class(const JKArgs& args, cudaStream_t stream) {
+  if (args.nwork <= 0) return 0;
+  using P = Policy<LA, LB, LC, LD>;
+  if constexpr (P::REG) {
+    jk_reg_kernel<LA, LB, LC, LD, R><<<args.nwork, 128, 0, stream>>>(args);
+  } else {
+    constexpr int TEAM = P::TEAM;
+    using SM = TeamSmem<LA, LB, LC, LD, R, TEAM>;
+    constexpr size_t per_team = SM::bytes();
+    int teams = 128 / TEAM;
+    while (teams > 1 && per_team * teams > 200 * 1024) --teams;
+    const size_t smem = per_team * teams;
+    if (smem > 48 * 1024) {
+      static bool configured = false;
+      if (!configured) {
+        cudaFuncSetAttribute(jk_team_kernel<LA, LB, LC, LD, R, TEAM>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        configured = true;
+      }
+    }
+    jk_team_kernel<LA, LB, LC, LD, R, TEAM><<<args.nwork, teams * TEAM, smem, stream>>>(args);
+  }
+  return (int)cudaGetLastError();
+}
+
+#if BRA_CLASS == KET_CLASS
+template <int LA, int LB>
+int launch_schwarz(const JKArgs& args, int npairs, int cart, cudaStream_t stream) {
+  if (npairs <= 0) return 0;
+  constexpr int TEAM = Policy<LA, LB, LA, LB>::TEAM;
+  using SM = TeamSmem<LA, LB, LA, LB, double, TEAM>;
+  constexpr size_t per_team = SM::bytes();
+  int teams = 128 / TEAM;
+  while (teams > 1 && per_team * teams > 200 * 1024) --teams;
+  const size_t smem = per_team * teams;
+  if (smem > 48 * 1024) {
+    static bool configured = false;
+    if (!configured) {
+      cudaFuncSetAttribute(schwarz_kernel<LA, LB, TEAM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      configured = true;
+    }
+  }
+  const int blocks = (npairs + teams - 1) / teams;
+  schwarz_kernel<LA, LB, TEAM><<<blocks, teams * TEAM, smem, stream>>>(args, npairs, cart);
+  return (int)cudaGetLastError();
+}
+#endif
+
+constexpr int X = BRA_CLASS;
+constexpr int Y = KET_CLASS;
+static_assert(Y <= X, "ket class must not exceed bra class");
+constexpr int XA = pc_la(X), XB = pc_lb(X);
+constexpr int YA = pc_la(Y), YB = pc_lb(Y);
+
+}  // namespace
+
+#define CAT4(a, b, c, d) a##b##c##d
+#define REG_NAME(x, y) CAT4(register_jk_class_, x, _, y)
+void REG_NAME(BRA_CLASS, KET_CLASS)(DispatchTable& t) {
+  const int id = X * (X + 1) / 2 + Y;
+  t.jk64[id] = &launch_class<XA, XB, YA, YB, double>;
+  t.jk32[id] = &launch_class<XA, XB, YA, YB, float>;
+  t.reg_path[id] = Policy<XA, XB, YA, YB>::REG;
+  t.team[id] = Policy<XA, XB, YA, YB>::REG ? 1 : Policy<XA, XB, YA, YB>::TEAM;
+#if BRA_CLASS == KET_CLASS
+  t.schwarz[X] = &launch_schwarz<XA, XB>;
+#endif
+}
+
+}  // namespace b200jk

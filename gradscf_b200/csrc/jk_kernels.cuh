@@ -1,0 +1,585 @@
+// Direct J/K shell-quartet kernels, one template instantiation per
+// angular-momentum class (LA>=LB | LC>=LD), FP64 or FP32 arithmetic.
+//
+// Work decomposition: the significant shell pairs of one pair class are
+// sorted by Schwarz bound (descending) -- the "bra list"; for a class pair
+// (X,Y) every bra pair p of X meets the leading kets of Y whose bound passes
+// Q_p Q_q >= cut (and q <= p when X == Y).  A work item is (bra position,
+// ket range); one CUDA block takes one item.
+//
+// Digestion (all in the raw Cartesian basis, densities pre-transformed):
+// with s = (A==B ? 1/2:1)(C==D ? 1/2:1)(pq ? 1/2:1) the unique quartet adds
+//   MJ[a][b] += 2s sum_cd V D_cd,   MJ[c][d] += 2s sum_ab V D_ab,
+//   MK[a][c] += s sum_bd V D_bd,    MK[a][d] += s sum_bc V D_bc,
+//   MK[b][c] += s sum_ad V D_ad,    MK[b][d] += s sum_ac V D_ac,
+// and the caller finalises J = MJ + MJ^T, K = MK +/- MK^T (symmetric /
+// antisymmetric density part).  That is the reference's eight-permutation
+// scatter (csrc/direct_jk.cc:50-75) folded by the symmetry of D.
+#pragma once
+#include "common.cuh"
+
+namespace b200jk {
+
+struct JKArgs {
+  const int4* sh_info;       // (cart offset in molecule, l, molecule, unused)
+  const double4* sh_xyz;     // centre
+  const int4* pair_info;     // (shell A, shell B, first primitive pair, count)
+  const double4* pp_data;    // primitive pair: (Px, Py, Pz, p = a+b)
+  const double* pp_k;        // exp(-ab/p |AB|^2) * c_a * c_b
+  const long long* mol_base; // offset of the molecule's n x n block
+  const int* mol_n;          // Cartesian AO count of the molecule
+  const int* bra_pairs;      // sorted pair ids of the bra class
+  const int* ket_pairs;      // sorted pair ids of the ket class
+  const int4* work;          // (bra position, ket begin, ket end, unused)
+  int nwork;
+  const int* split;          // per bra position: first ket computed in FP32
+  int split_mode;            // 0 all kets, 1 kets below split, 2 kets from split
+  const double* dens;        // [ndm][dstride] Cartesian effective densities
+  double* vj;                // [nsym][dstride]
+  double* vk;                // [ndm][dstride]
+  long long dstride;
+  int ndm, nsym, with_j, with_k;
+  Tables tb;
+  double* q_out;             // Schwarz mode: per pair max |(ab|ab)| in output basis
+  int* status;               // device error word (0 = ok)
+};
+
+template <int LA, int LB, int LC, int LD>
+struct GIdx {
+  __host__ __device__ static constexpr int idx(int a, int b, int c, int d) {
+    return ((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d;
+  }
+};
+
+// Ket range of a work item for the requested precision slice.
+__device__ __forceinline__ void ket_range(const JKArgs& args, const int4 w, int& kb, int& ke) {
+  kb = w.y;
+  ke = w.z;
+  if (args.split_mode != 0) {
+    const int s = args.split[w.x];
+    if (args.split_mode == 1) ke = min(ke, s);
+    else kb = max(kb, s);
+  }
+}
+
+// Quartet-level geometry shared by both paths.
+struct QuartetGeom {
+  int A, B, C, D;
+  int ppa, npa, ppc, npc;
+  double ax, ay, az, cx, cy, cz;
+  double abx, aby, abz, cdx, cdy, cdz;
+  int aoA, aoB, aoC, aoD, mol;
+  double scale;
+};
+
+__device__ __forceinline__ void load_quartet(const JKArgs& args, int bra, int ket, QuartetGeom& g) {
+  const int4 pb = args.pair_info[bra];
+  const int4 pk = args.pair_info[ket];
+  g.A = pb.x; g.B = pb.y; g.ppa = pb.z; g.npa = pb.w;
+  g.C = pk.x; g.D = pk.y; g.ppc = pk.z; g.npc = pk.w;
+  const double4 ra = args.sh_xyz[g.A], rb = args.sh_xyz[g.B];
+  const double4 rc = args.sh_xyz[g.C], rd = args.sh_xyz[g.D];
+  g.ax = ra.x; g.ay = ra.y; g.az = ra.z;
+  g.cx = rc.x; g.cy = rc.y; g.cz = rc.z;
+  g.abx = ra.x - rb.x; g.aby = ra.y - rb.y; g.abz = ra.z - rb.z;
+  g.cdx = rc.x - rd.x; g.cdy = rc.y - rd.y; g.cdz = rc.z - rd.z;
+  const int4 ia = args.sh_info[g.A], ib = args.sh_info[g.B];
+  const int4 ic = args.sh_info[g.C], id = args.sh_info[g.D];
+  g.aoA = ia.x; g.aoB = ib.x; g.aoC = ic.x; g.aoD = id.x; g.mol = ia.z;
+  double s = 1.0;
+  if (g.A == g.B) s *= 0.5;
+  if (g.C == g.D) s *= 0.5;
+  if (bra == ket) s *= 0.5;
+  g.scale = s;
+}
+
+// Per primitive quartet scalars.
+template <typename R>
+struct PrimQ {
+  R pq_inv, q_pq, p_pq;      // 1/(p+q), q/(p+q), p/(p+q)
+  R inv2p, inv2q;            // 1/(2p), 1/(2q)
+  R pax, pay, paz, qcx, qcy, qcz, pqx, pqy, pqz;
+  R t, pref;
+};
+
+template <typename R>
+__device__ __forceinline__ void prim_setup(const JKArgs& args, const QuartetGeom& g, int i, int j,
+                                           PrimQ<R>& s) {
+  const double4 P = args.pp_data[i];
+  const double4 Q = args.pp_data[j];
+  const double kab = args.pp_k[i], kcd = args.pp_k[j];
+  const double p = P.w, q = Q.w;
+  const double pq = p + q;
+  const double pqx = P.x - Q.x, pqy = P.y - Q.y, pqz = P.z - Q.z;
+  const double rho = p * q / pq;
+  const double t = rho * (pqx * pqx + pqy * pqy + pqz * pqz);
+  s.t = R(t);
+  s.pref = R(B200JK_ERI_C0 * kab * kcd / (p * q * sqrt(pq)));
+  s.pq_inv = R(1.0 / pq);
+  s.q_pq = R(q / pq);
+  s.p_pq = R(p / pq);
+  s.inv2p = R(0.5 / p);
+  s.inv2q = R(0.5 / q);
+  s.pax = R(P.x - g.ax); s.pay = R(P.y - g.ay); s.paz = R(P.z - g.az);
+  s.qcx = R(Q.x - g.cx); s.qcy = R(Q.y - g.cy); s.qcz = R(Q.z - g.cz);
+  s.pqx = R(pqx); s.pqy = R(pqy); s.pqz = R(pqz);
+}
+
+// Rys coefficients of one root for the three axes.
+template <typename R>
+struct RootCoef {
+  R b00, b10, b01;
+  R c00[3], c0p[3];
+};
+
+template <typename R>
+__device__ __forceinline__ void root_coef(const PrimQ<R>& s, R u, RootCoef<R>& rc) {
+  const R up = u * s.pq_inv;
+  rc.b00 = R(0.5) * up;
+  rc.b10 = s.inv2p - s.inv2p * u * s.q_pq;
+  rc.b01 = s.inv2q - s.inv2q * u * s.p_pq;
+  const R uq = u * s.q_pq, upp = u * s.p_pq;
+  rc.c00[0] = s.pax - uq * s.pqx;
+  rc.c00[1] = s.pay - uq * s.pqy;
+  rc.c00[2] = s.paz - uq * s.pqz;
+  rc.c0p[0] = s.qcx + upp * s.pqx;
+  rc.c0p[1] = s.qcy + upp * s.pqy;
+  rc.c0p[2] = s.qcz + upp * s.pqz;
+}
+
+__device__ __forceinline__ long long dm_index(const JKArgs& args, int mol, int a, int b) {
+  return args.mol_base[mol] + (long long)a * args.mol_n[mol] + b;
+}
+
+// ---------------------------------------------------------------------------
+// Register path: one thread per quartet, the whole Cartesian block in registers.
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const QuartetGeom& g,
+                                                  R* out) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using GI = GIdx<LA, LB, LC, LD>;
+  constexpr int N = CI::NROOT;
+#pragma unroll
+  for (int o = 0; o < CI::NOUT; ++o) out[o] = R(0);
+  for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
+    for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
+      PrimQ<R> s;
+      prim_setup<R>(args, g, i, j, s);
+      R x[N], w[N];
+      rys_roots<N, R>(s.t, x, w, args.tb);
+#pragma unroll
+      for (int r = 0; r < N; ++r) {
+        RootCoef<R> rc;
+        root_coef<R>(s, x[r], rc);
+        R gx[CI::NG], gy[CI::NG], gz[CI::NG];
+        build_g<LA, LB, LC, LD, R>(rc.c00[0], rc.c0p[0], rc.b10, rc.b01, rc.b00, R(1), R(g.abx),
+                                   R(g.cdx), gx);
+        build_g<LA, LB, LC, LD, R>(rc.c00[1], rc.c0p[1], rc.b10, rc.b01, rc.b00, R(1), R(g.aby),
+                                   R(g.cdy), gy);
+        build_g<LA, LB, LC, LD, R>(rc.c00[2], rc.c0p[2], rc.b10, rc.b01, rc.b00, w[r] * s.pref,
+                                   R(g.abz), R(g.cdz), gz);
+#pragma unroll
+        for (int ia = 0; ia < CI::NA; ++ia)
+#pragma unroll
+          for (int ib = 0; ib < CI::NB; ++ib)
+#pragma unroll
+            for (int ic = 0; ic < CI::NC; ++ic)
+#pragma unroll
+              for (int id = 0; id < CI::ND; ++id) {
+                const int o = ((ia * CI::NB + ib) * CI::NC + ic) * CI::ND + id;
+                const int jx = GI::idx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
+                const int jy = GI::idx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
+                const int jz = GI::idx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
+                out[o] += gx[jx] * gy[jy] * gz[jz];
+              }
+      }
+    }
+  }
+}
+
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom& g, const R* out) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  constexpr int NA = CI::NA, NB = CI::NB, NC = CI::NC, ND = CI::ND;
+  const double s = g.scale;
+  const long long base = args.mol_base[g.mol];
+  const int n = args.mol_n[g.mol];
+  for (int e = 0; e < args.ndm; ++e) {
+    const double* dm = args.dens + e * args.dstride + base;
+    if (args.with_j && e < args.nsym) {
+      double* vj = args.vj + e * args.dstride + base;
+      double dab[NA * NB], dcd[NC * ND];
+#pragma unroll
+      for (int a = 0; a < NA; ++a)
+#pragma unroll
+        for (int b = 0; b < NB; ++b) dab[a * NB + b] = dm[(long long)(g.aoA + a) * n + g.aoB + b];
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int d = 0; d < ND; ++d) dcd[c * ND + d] = dm[(long long)(g.aoC + c) * n + g.aoD + d];
+#pragma unroll
+      for (int ab = 0; ab < NA * NB; ++ab) {
+        double acc = 0.0;
+#pragma unroll
+        for (int cd = 0; cd < NC * ND; ++cd) acc += double(out[ab * NC * ND + cd]) * dcd[cd];
+        atomicAdd(vj + (long long)(g.aoA + ab / NB) * n + g.aoB + ab % NB, 2.0 * s * acc);
+      }
+#pragma unroll
+      for (int cd = 0; cd < NC * ND; ++cd) {
+        double acc = 0.0;
+#pragma unroll
+        for (int ab = 0; ab < NA * NB; ++ab) acc += double(out[ab * NC * ND + cd]) * dab[ab];
+        atomicAdd(vj + (long long)(g.aoC + cd / ND) * n + g.aoD + cd % ND, 2.0 * s * acc);
+      }
+    }
+    if (args.with_k) {
+      double* vk = args.vk + e * args.dstride + base;
+      // K[a][c] += s sum_bd V D[b][d]
+      {
+        double dbd[NB * ND];
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+#pragma unroll
+          for (int d = 0; d < ND; ++d) dbd[b * ND + d] = dm[(long long)(g.aoB + b) * n + g.aoD + d];
+#pragma unroll
+        for (int a = 0; a < NA; ++a)
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            double acc = 0.0;
+#pragma unroll
+            for (int b = 0; b < NB; ++b)
+#pragma unroll
+              for (int d = 0; d < ND; ++d)
+                acc += double(out[((a * NB + b) * NC + c) * ND + d]) * dbd[b * ND + d];
+            atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoC + c, s * acc);
+          }
+      }
+      // K[a][d] += s sum_bc V D[b][c]
+      {
+        double dbc[NB * NC];
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+#pragma unroll
+          for (int c = 0; c < NC; ++c) dbc[b * NC + c] = dm[(long long)(g.aoB + b) * n + g.aoC + c];
+#pragma unroll
+        for (int a = 0; a < NA; ++a)
+#pragma unroll
+          for (int d = 0; d < ND; ++d) {
+            double acc = 0.0;
+#pragma unroll
+            for (int b = 0; b < NB; ++b)
+#pragma unroll
+              for (int c = 0; c < NC; ++c)
+                acc += double(out[((a * NB + b) * NC + c) * ND + d]) * dbc[b * NC + c];
+            atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoD + d, s * acc);
+          }
+      }
+      // K[b][c] += s sum_ad V D[a][d]
+      {
+        double dad[NA * ND];
+#pragma unroll
+        for (int a = 0; a < NA; ++a)
+#pragma unroll
+          for (int d = 0; d < ND; ++d) dad[a * ND + d] = dm[(long long)(g.aoA + a) * n + g.aoD + d];
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            double acc = 0.0;
+#pragma unroll
+            for (int a = 0; a < NA; ++a)
+#pragma unroll
+              for (int d = 0; d < ND; ++d)
+                acc += double(out[((a * NB + b) * NC + c) * ND + d]) * dad[a * ND + d];
+            atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoC + c, s * acc);
+          }
+      }
+      // K[b][d] += s sum_ac V D[a][c]
+      {
+        double dac[NA * NC];
+#pragma unroll
+        for (int a = 0; a < NA; ++a)
+#pragma unroll
+          for (int c = 0; c < NC; ++c) dac[a * NC + c] = dm[(long long)(g.aoA + a) * n + g.aoC + c];
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+#pragma unroll
+          for (int d = 0; d < ND; ++d) {
+            double acc = 0.0;
+#pragma unroll
+            for (int a = 0; a < NA; ++a)
+#pragma unroll
+              for (int c = 0; c < NC; ++c)
+                acc += double(out[((a * NB + b) * NC + c) * ND + d]) * dac[a * NC + c];
+            atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoD + d, s * acc);
+          }
+      }
+    }
+  }
+}
+
+template <int LA, int LB, int LC, int LD, typename R>
+__global__ void __launch_bounds__(128) jk_reg_kernel(JKArgs args) {
+  const int4 w = args.work[blockIdx.x];
+  int kb, ke;
+  ket_range(args, w, kb, ke);
+  const int bra = args.bra_pairs[w.x];
+  for (int k = kb + threadIdx.x; k < ke; k += blockDim.x) {
+    QuartetGeom g;
+    load_quartet(args, bra, args.ket_pairs[k], g);
+    R out[ClassInfo<LA, LB, LC, LD>::NOUT];
+    quartet_block_reg<LA, LB, LC, LD, R>(args, g, out);
+    digest_reg<LA, LB, LC, LD, R>(args, g, out);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Team path: TEAM lanes of one warp share a quartet.  Rys functions and the
+// 3*NROOT (root, axis) 2D-integral tables are built cooperatively in shared
+// memory; each lane accumulates a strided slice of the Cartesian block; the
+// contracted block is staged in shared memory for digestion (one atomic per
+// digested element).  Blocks larger than TEAM*NK are done in passes.
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD, int TEAM>
+struct TeamCfg {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  static constexpr int NK_MAX = 48;
+  static constexpr int NK = (CI::NOUT + TEAM - 1) / TEAM < NK_MAX ? (CI::NOUT + TEAM - 1) / TEAM : NK_MAX;
+  static constexpr int PASS = TEAM * NK;
+  static constexpr int NPASS = (CI::NOUT + PASS - 1) / PASS;
+  static constexpr int G_ELEMS = 3 * CI::NROOT * CI::NG;
+  static constexpr int ROOT_ELEMS = 2 * CI::NROOT;
+  // G region (+ roots) and the staged block V; V may alias G in one pass.
+  static constexpr int GR = G_ELEMS + ROOT_ELEMS;
+  static constexpr int ELEMS = NPASS == 1 ? (GR > CI::NOUT ? GR : CI::NOUT) : GR + CI::NOUT;
+};
+
+template <int LA, int LB, int LC, int LD, typename R, int TEAM>
+__device__ __forceinline__ void team_block(const JKArgs& args, const QuartetGeom& g, R* sm,
+                                           double* vsm, int lane, unsigned mask) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using TC = TeamCfg<LA, LB, LC, LD, TEAM>;
+  using GI = GIdx<LA, LB, LC, LD>;
+  constexpr int N = CI::NROOT;
+  constexpr int NG = CI::NG;
+  R* G = sm;
+  R* roots = sm + TC::G_ELEMS;
+  for (int pass = 0; pass < TC::NPASS; ++pass) {
+    R acc[TC::NK];
+    int ixyz[TC::NK];
+#pragma unroll
+    for (int k = 0; k < TC::NK; ++k) {
+      acc[k] = R(0);
+      const int o = pass * TC::PASS + lane + k * TEAM;
+      if (o < CI::NOUT) {
+        const int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
+        const int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
+        const int jx = GI::idx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
+        const int jy = GI::idx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
+        const int jz = GI::idx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
+        ixyz[k] = jx | (jy << 10) | (jz << 20);
+      } else {
+        ixyz[k] = -1;
+      }
+    }
+    for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
+      for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
+        PrimQ<R> s;
+        prim_setup<R>(args, g, i, j, s);
+        for (int f = lane; f < 2 * N; f += TEAM) roots[f] = rys_one<N, R>(s.t, f, args.tb);
+        __syncwarp(mask);
+        for (int tsk = lane; tsk < 3 * N; tsk += TEAM) {
+          const int r = tsk / 3, ax = tsk - 3 * r;
+          RootCoef<R> rc;
+          root_coef<R>(s, roots[r], rc);
+          const R abd = ax == 0 ? R(g.abx) : (ax == 1 ? R(g.aby) : R(g.abz));
+          const R cdd = ax == 0 ? R(g.cdx) : (ax == 1 ? R(g.cdy) : R(g.cdz));
+          const R g00 = ax == 2 ? roots[N + r] * s.pref : R(1);
+          build_g<LA, LB, LC, LD, R>(rc.c00[ax], rc.c0p[ax], rc.b10, rc.b01, rc.b00, g00, abd, cdd,
+                                     G + (r * 3 + ax) * NG);
+        }
+        __syncwarp(mask);
+#pragma unroll
+        for (int k = 0; k < TC::NK; ++k) {
+          if (ixyz[k] >= 0) {
+            const int jx = ixyz[k] & 1023, jy = (ixyz[k] >> 10) & 1023, jz = ixyz[k] >> 20;
+            R a = acc[k];
+#pragma unroll
+            for (int r = 0; r < N; ++r)
+              a += G[(r * 3) * NG + jx] * G[(r * 3 + 1) * NG + jy] * G[(r * 3 + 2) * NG + jz];
+            acc[k] = a;
+          }
+        }
+        __syncwarp(mask);
+      }
+    }
+    // stage this pass into V (double)
+#pragma unroll
+    for (int k = 0; k < TC::NK; ++k) {
+      const int o = pass * TC::PASS + lane + k * TEAM;
+      if (o < CI::NOUT) vsm[o] = double(acc[k]);
+    }
+    __syncwarp(mask);
+  }
+}
+
+template <int LA, int LB, int LC, int LD, int TEAM>
+__device__ __forceinline__ void team_digest(const JKArgs& args, const QuartetGeom& g,
+                                            const double* V, int lane) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  constexpr int NA = CI::NA, NB = CI::NB, NC = CI::NC, ND = CI::ND;
+  constexpr int T0 = NA * NB, T1 = T0 + NC * ND, T2 = T1 + NA * NC, T3 = T2 + NA * ND,
+                T4 = T3 + NB * NC, T5 = T4 + NB * ND;
+  const double s = g.scale;
+  const long long base = args.mol_base[g.mol];
+  const int n = args.mol_n[g.mol];
+  for (int e = 0; e < args.ndm; ++e) {
+    const double* dm = args.dens + e * args.dstride + base;
+    const bool doj = args.with_j && e < args.nsym;
+    double* vj = doj ? args.vj + e * args.dstride + base : nullptr;
+    double* vk = args.vk + e * args.dstride + base;
+    for (int t = lane; t < T5; t += TEAM) {
+      double acc = 0.0;
+      if (t < T1) {
+        if (!doj) continue;
+        if (t < T0) {
+          const int a = t / NB, b = t % NB;
+          for (int c = 0; c < NC; ++c)
+            for (int d = 0; d < ND; ++d)
+              acc += V[((a * NB + b) * NC + c) * ND + d] * dm[(long long)(g.aoC + c) * n + g.aoD + d];
+          atomicAdd(vj + (long long)(g.aoA + a) * n + g.aoB + b, 2.0 * s * acc);
+        } else {
+          const int c = (t - T0) / ND, d = (t - T0) % ND;
+          for (int a = 0; a < NA; ++a)
+            for (int b = 0; b < NB; ++b)
+              acc += V[((a * NB + b) * NC + c) * ND + d] * dm[(long long)(g.aoA + a) * n + g.aoB + b];
+          atomicAdd(vj + (long long)(g.aoC + c) * n + g.aoD + d, 2.0 * s * acc);
+        }
+        continue;
+      }
+      if (!args.with_k) continue;
+      if (t < T2) {
+        const int a = (t - T1) / NC, c = (t - T1) % NC;
+        for (int b = 0; b < NB; ++b)
+          for (int d = 0; d < ND; ++d)
+            acc += V[((a * NB + b) * NC + c) * ND + d] * dm[(long long)(g.aoB + b) * n + g.aoD + d];
+        atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoC + c, s * acc);
+      } else if (t < T3) {
+        const int a = (t - T2) / ND, d = (t - T2) % ND;
+        for (int b = 0; b < NB; ++b)
+          for (int c = 0; c < NC; ++c)
+            acc += V[((a * NB + b) * NC + c) * ND + d] * dm[(long long)(g.aoB + b) * n + g.aoC + c];
+        atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoD + d, s * acc);
+      } else if (t < T4) {
+        const int b = (t - T3) / NC, c = (t - T3) % NC;
+        for (int a = 0; a < NA; ++a)
+          for (int d = 0; d < ND; ++d)
+            acc += V[((a * NB + b) * NC + c) * ND + d] * dm[(long long)(g.aoA + a) * n + g.aoD + d];
+        atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoC + c, s * acc);
+      } else {
+        const int b = (t - T4) / ND, d = (t - T4) % ND;
+        for (int a = 0; a < NA; ++a)
+          for (int c = 0; c < NC; ++c)
+            acc += V[((a * NB + b) * NC + c) * ND + d] * dm[(long long)(g.aoA + a) * n + g.aoC + c];
+        atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoD + d, s * acc);
+      }
+    }
+  }
+}
+
+template <int LA, int LB, int LC, int LD, typename R, int TEAM>
+struct TeamSmem {
+  using TC = TeamCfg<LA, LB, LC, LD, TEAM>;
+  // bytes per team: R-typed G/roots region, then (if not aliased) a double V region
+  __host__ __device__ static constexpr size_t bytes() {
+    return TC::NPASS == 1
+               ? ((size_t)TC::GR * sizeof(R) > (size_t)ClassInfo<LA, LB, LC, LD>::NOUT * 8
+                      ? (size_t)TC::GR * sizeof(R)
+                      : (size_t)ClassInfo<LA, LB, LC, LD>::NOUT * 8)
+               : (((size_t)TC::GR * sizeof(R) + 15) / 16) * 16 +
+                     (size_t)ClassInfo<LA, LB, LC, LD>::NOUT * 8;
+  }
+  __host__ __device__ static constexpr size_t vofs() {
+    return TC::NPASS == 1 ? 0 : (((size_t)TC::GR * sizeof(R) + 15) / 16) * 16;
+  }
+};
+
+template <int LA, int LB, int LC, int LD, typename R, int TEAM>
+__global__ void jk_team_kernel(JKArgs args) {
+  using SM = TeamSmem<LA, LB, LC, LD, R, TEAM>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x % TEAM;
+  const int team = threadIdx.x / TEAM;
+  const int nteams = blockDim.x / TEAM;
+  const unsigned mask =
+      TEAM == 32 ? 0xffffffffu : (((1u << TEAM) - 1u) << ((threadIdx.x % 32) / TEAM * TEAM));
+  unsigned char* mine = smem_raw + (size_t)team * SM::bytes();
+  R* sm = reinterpret_cast<R*>(mine);
+  double* vsm = reinterpret_cast<double*>(mine + SM::vofs());
+  const int4 w = args.work[blockIdx.x];
+  int kb, ke;
+  ket_range(args, w, kb, ke);
+  const int bra = args.bra_pairs[w.x];
+  for (int k = kb + team; k < ke; k += nteams) {
+    QuartetGeom g;
+    load_quartet(args, bra, args.ket_pairs[k], g);
+    team_block<LA, LB, LC, LD, R, TEAM>(args, g, sm, vsm, lane, mask);
+    team_digest<LA, LB, LC, LD, TEAM>(args, g, vsm, lane);
+    __syncwarp(mask);
+  }
+}
+
+// Schwarz bound of one work pair: max over output-basis AO pairs (a,b) of
+// |(ab|ab)| (csrc/coulomb_shells.h:60-77 uses the same diagonal), one team
+// per pair.  c2s[l] holds the 10x7 output transform of shell l.
+template <int LA, int LB, int TEAM>
+__global__ void schwarz_kernel(JKArgs args, int npairs, int cart) {
+  using SM = TeamSmem<LA, LB, LA, LB, double, TEAM>;
+  using CI = ClassInfo<LA, LB, LA, LB>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x % TEAM;
+  const int team = threadIdx.x / TEAM;
+  const int nteams = blockDim.x / TEAM;
+  const unsigned mask =
+      TEAM == 32 ? 0xffffffffu : (((1u << TEAM) - 1u) << ((threadIdx.x % 32) / TEAM * TEAM));
+  unsigned char* mine = smem_raw + (size_t)team * SM::bytes();
+  double* sm = reinterpret_cast<double*>(mine);
+  double* V = reinterpret_cast<double*>(mine + SM::vofs());
+  const int pos = blockIdx.x * nteams + team;
+  if (pos >= npairs) return;
+  const int pair = args.bra_pairs[pos];
+  QuartetGeom g;
+  load_quartet(args, pair, pair, g);
+  team_block<LA, LB, LA, LB, double, TEAM>(args, g, sm, V, lane, mask);
+  const int nfa = cart ? CI::NA : 2 * LA + 1, nfb = cart ? CI::NB : 2 * LB + 1;
+  const double* ta = args.tb.c2s + LA * kTS;
+  const double* tb = args.tb.c2s + LB * kTS;
+  double best = 0.0;
+  for (int t = lane; t < nfa * nfb; t += TEAM) {
+    const int fa = t / nfb, fb = t % nfb;
+    double acc = 0.0;
+    for (int a1 = 0; a1 < CI::NA; ++a1) {
+      const double x1 = ta[a1 * kTW + fa];
+      if (x1 == 0.0) continue;
+      for (int b1 = 0; b1 < CI::NB; ++b1) {
+        const double y1 = tb[b1 * kTW + fb];
+        if (y1 == 0.0) continue;
+        for (int a2 = 0; a2 < CI::NA; ++a2) {
+          const double x2 = ta[a2 * kTW + fa];
+          if (x2 == 0.0) continue;
+          for (int b2 = 0; b2 < CI::NB; ++b2) {
+            const double y2 = tb[b2 * kTW + fb];
+            if (y2 == 0.0) continue;
+            acc += x1 * y1 * x2 * y2 * V[((a1 * CI::NB + b1) * CI::NA + a2) * CI::NB + b2];
+          }
+        }
+      }
+    }
+    best = fmax(best, fabs(acc));
+  }
+  for (int off = TEAM / 2; off > 0; off >>= 1) best = fmax(best, __shfl_down_sync(mask, best, off, TEAM));
+  if (lane == 0) args.q_out[pair] = best;
+}
+
+}  // namespace b200jk

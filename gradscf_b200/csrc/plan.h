@@ -1,0 +1,98 @@
+// Host-side plan: the device-resident description of one batch of molecules.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "dispatch.h"
+
+namespace b200jk {
+
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes && ptr) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&ptr, n > 0 ? n : 16);
+    if (e == cudaSuccess) bytes = n;
+    return e;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+struct ClassPairWork {
+  int x = 0, y = 0;             // bra / ket pair classes
+  int nwork = 0;
+  int nbra = 0;
+  DevBuf work;                  // int4 per work item
+  DevBuf bra_kets;              // int2 per bra position: [ket lo, ket hi)
+  DevBuf split;                 // int per bra position (filled per call)
+  long long quartets = 0;       // significant quartets in this class pair
+};
+
+struct ClassList {
+  std::vector<int> pairs;       // pair ids, sorted (molecule, Q desc)
+  std::vector<double> q;        // their parent Schwarz bounds
+  std::vector<int> mol_begin;   // per molecule: first position (size nmol+1)
+  DevBuf d_pairs, d_q;
+};
+
+struct Plan {
+  int device = 0;
+  int cart = 0;
+  double cutoff = 0.0;
+  int nmol = 0;
+  // per molecule
+  std::vector<int> mol_nout, mol_ncart, mol_natm, mol_atm_off;
+  std::vector<long long> mol_out_base, mol_cart_base;
+  long long out_stride = 0, cart_stride = 0;
+  int total_atm = 0;
+  // work shells
+  int nws = 0;
+  std::vector<int4> ws_info;     // (cart offset in mol, l, mol, out offset in mol)
+  std::vector<double4> ws_xyz;
+  std::vector<int> ws_parent;    // global parent shell id
+  std::vector<int> ws_atm;       // global atm row of the shell's centre
+  std::vector<int> ws_nprim;
+  std::vector<double> ws_exp, ws_coef;  // per primitive (flattened), coef of this column
+  std::vector<int> ws_prim_off;
+  // pairs
+  int npair = 0;
+  std::vector<int4> pair_info;   // (A, B, pp offset, pp count)
+  std::vector<int> pair_class;
+  std::vector<double> pair_q;    // parent Schwarz bound
+  ClassList classes[kPairClasses];
+  std::vector<ClassPairWork*> work;
+  long long quartets = 0;
+  // nuclei (for one-electron terms): global atm rows with charge
+  std::vector<double4> atom_xyzq; // (x, y, z, charge) per global atm row
+  // device tables
+  DevBuf d_ws_info, d_ws_xyz, d_pair_info, d_pp_data, d_pp_k, d_mol_base_cart, d_mol_ncart,
+      d_mol_base_out, d_mol_nout, d_cart_ws, d_out_ws, d_status, d_maxd, d_q_work, d_atoms,
+      d_ws_atm, d_mol_ao_off, d_ws_prim, d_ws_prim_off;
+  // scratch
+  DevBuf d_dens, d_vj, d_vk;
+  int scratch_nb = 0;
+  ~Plan() {
+    for (auto* w : work) delete w;
+  }
+};
+
+// Device-wide constant tables (Rys, Boys, c2s) of the current device.
+const Tables& device_tables(int device);
+
+void set_error(const std::string& msg);
+
+}  // namespace b200jk

@@ -1,0 +1,230 @@
+"""Direct J/K on the B200 through the C ABI, mirroring the reference's API.
+
+Reference surface mirrored here (src/gradscf/integrals/...):
+  * ``direct_jk(atm, bas, env, density, *, cart, cutoff, workers, with_j,
+    with_k)`` -- backends/native/jk.py:399-446: (..., n, n) float64 or
+    complex128 densities, complex split into real/imag batches, returns (J, K)
+    with zeros for an operator that was not requested.
+  * ``IntegralPlan.get_jk`` -- plan.py:71-92, ``make_plan`` -- plan.py:185-190.
+  * ``NativeDirectBasis.get_jk`` -- backends/native/jk.py:98-107.
+Arrays are torch tensors on a CUDA device (numpy inputs are moved there).
+"""
+from __future__ import annotations
+
+import ctypes
+from collections import OrderedDict
+from dataclasses import dataclass
+from numbers import Integral
+
+import numpy as np
+import torch
+
+from . import _capi
+from .basis import BasisParameters, BasisTopology, build_tables, pack
+
+PRECISIONS = {"fp64": _capi.FP64, "split": _capi.SPLIT}
+DEFAULT_FP32_CUT = 1e-6
+
+
+def _stream_handle(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+class DirectJKPlan:
+    """Device-resident plan (``b200jk_plan_create``) for one molecule or a batch.
+
+    ``molecules`` is a sequence of (atm, bas, env) libcint tables.  Densities
+    and results use the packed layout: molecule m occupies
+    ``[offsets[m], offsets[m] + nao[m]**2)`` of every matrix.
+    """
+
+    def __init__(self, molecules, *, cart, cutoff=0.0, device=None):
+        lib = _capi.lib()
+        dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        if dev.type != "cuda":
+            raise ValueError("DirectJKPlan needs a CUDA device")
+        self.device = dev
+        self.cart = bool(cart)
+        self.cutoff = float(cutoff)
+        keep = []
+        arr = (_capi.Molecule * len(molecules))()
+        for i, (atm, bas, env) in enumerate(molecules):
+            a = np.ascontiguousarray(atm, dtype=np.int32)
+            b = np.ascontiguousarray(bas, dtype=np.int32)
+            e = np.ascontiguousarray(env, dtype=np.float64)
+            keep += [a, b, e]
+            arr[i] = _capi.Molecule(a.ctypes.data, a.shape[0], b.ctypes.data, b.shape[0],
+                                    e.ctypes.data, e.shape[0])
+        self.natm = [int(np.asarray(m[0]).shape[0]) for m in molecules]
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(dev):
+            _capi.check(lib.b200jk_plan_create(arr, len(molecules), int(cart), float(cutoff),
+                                               dev.index or 0, ctypes.byref(handle)))
+        self._h = handle
+        self.nmol = len(molecules)
+        n = ctypes.c_int32()
+        self.nao = []
+        for m in range(self.nmol):
+            _capi.check(lib.b200jk_plan_nao(self._h, m, ctypes.byref(n)))
+            self.nao.append(n.value)
+        offs = (ctypes.c_int64 * self.nmol)()
+        _capi.check(lib.b200jk_plan_block_offsets(self._h, offs))
+        self.offsets = list(offs)
+        self.packed_size = self.offsets[-1] + self.nao[-1] ** 2
+        q = ctypes.c_int64()
+        _capi.check(lib.b200jk_plan_quartets(self._h, ctypes.byref(q)))
+        self.quartets = q.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _capi.lib().b200jk_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- J/K ---------------------------------------------------------------
+    def jk_packed(self, density, *, with_j=True, with_k=True, hermi=0, precision="fp64",
+                  fp32_cut=DEFAULT_FP32_CUT, out=None, stream=None, check=True):
+        """density: (nb, packed_size) float64 CUDA tensor -> (nops, nb, packed_size)."""
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        d = density
+        if d.dtype != torch.float64 or d.device != self.device or d.dim() != 2 or d.shape[1] != self.packed_size:
+            raise ValueError("density must be a float64 (nb, packed_size) tensor on the plan's device")
+        d = d.contiguous()
+        nb = d.shape[0]
+        nops = int(bool(with_j)) + int(bool(with_k))
+        if out is None:
+            out = torch.empty((nops, nb, self.packed_size), dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            st = _stream_handle(stream)
+            _capi.check(_capi.lib().b200jk_direct_jk(
+                self._h, ctypes.c_void_p(d.data_ptr()), nb, ctypes.c_void_p(out.data_ptr()),
+                int(bool(with_j)), int(bool(with_k)), int(bool(hermi)), PRECISIONS[precision],
+                float(fp32_cut), st))
+            if check:
+                _capi.check(_capi.lib().b200jk_check_status(self._h, st))
+        return out
+
+    def jk(self, density, *, with_j=True, with_k=True, hermi=None, precision="fp64",
+           fp32_cut=DEFAULT_FP32_CUT, stream=None):
+        """Single-molecule convenience: (..., n, n) -> (J, K) of the same shape."""
+        if self.nmol != 1:
+            raise ValueError("jk() is for one-molecule plans; use jk_packed for batches")
+        n = self.nao[0]
+        d = torch.as_tensor(density, dtype=torch.float64, device=self.device)
+        shape = d.shape
+        if shape[-2:] != (n, n):
+            raise ValueError("Density AO dimensions do not match the plan.")
+        flat = d.reshape(-1, n * n)
+        if hermi is None:
+            hermi = bool(torch.equal(d, d.transpose(-1, -2)))
+        out = self.jk_packed(flat, with_j=with_j, with_k=with_k, hermi=hermi, precision=precision,
+                             fp32_cut=fp32_cut, stream=stream)
+        j = out[0].reshape(shape) if with_j else torch.zeros_like(d)
+        k = out[-1].reshape(shape) if with_k else torch.zeros_like(d)
+        return j, k
+
+
+_PLAN_CACHE: "OrderedDict[tuple, DirectJKPlan]" = OrderedDict()
+
+
+def cached_plan(atm, bas, env, *, cart, cutoff, device=None):
+    """Plans keyed by table contents (coordinates included), LRU of 8."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    a = np.ascontiguousarray(atm, dtype=np.int32)
+    b = np.ascontiguousarray(bas, dtype=np.int32)
+    e = np.ascontiguousarray(env, dtype=np.float64)
+    key = (a.tobytes(), b.tobytes(), e.tobytes(), bool(cart), float(cutoff), str(dev))
+    plan = _PLAN_CACHE.get(key)
+    if plan is None:
+        plan = DirectJKPlan([(a, b, e)], cart=cart, cutoff=cutoff, device=dev)
+        _PLAN_CACHE[key] = plan
+        while len(_PLAN_CACHE) > 8:
+            _PLAN_CACHE.popitem(last=False)
+    else:
+        _PLAN_CACHE.move_to_end(key)
+    return plan
+
+
+def direct_jk(atm, bas, env, density, *, cart, cutoff=0.0, workers=1, with_j=True, with_k=True,
+              precision="fp64", fp32_cut=DEFAULT_FP32_CUT, device=None):
+    """Contract J/K (backends/native/jk.py:399-446) on the GPU; returns (J, K)."""
+    if not all(isinstance(f, (bool, np.bool_)) for f in (with_j, with_k)):
+        raise ValueError("with_j and with_k must be static booleans.")
+    if isinstance(workers, bool) or not isinstance(workers, Integral) or workers < 1:
+        raise ValueError("workers must be a positive integer.")
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    d = torch.as_tensor(density, device=dev)
+    n = d.shape[-1]
+    if d.dim() < 2 or d.shape[-2:] != (n, n) or d.dtype not in (torch.float64, torch.complex128):
+        raise ValueError("Direct J/K requires (...,n,n) float64/complex128 density.")
+    if np.asarray(env).dtype != np.float64:
+        raise ValueError("Direct J/K requires float64 environment.")
+    if not (with_j or with_k):
+        return torch.zeros_like(d), torch.zeros_like(d)
+    plan = cached_plan(atm, bas, env, cart=cart, cutoff=cutoff, device=dev)
+    if plan.nao[0] != n:
+        raise ValueError("Direct J/K shape mismatch")
+    flat = d.reshape(-1, n, n)
+    count = flat.shape[0]
+    real = torch.cat((flat.real, flat.imag), 0) if d.is_complex() else flat
+    hermi = bool(torch.equal(real, real.transpose(-1, -2)))
+    out = plan.jk_packed(real.reshape(real.shape[0], n * n).contiguous(), with_j=bool(with_j),
+                         with_k=bool(with_k), hermi=hermi, precision=precision, fp32_cut=fp32_cut)
+    out = out.reshape(out.shape[0], -1, n, n)
+    if d.is_complex():
+        out = torch.complex(out[:, :count], out[:, count:])
+    out = out.reshape(int(with_j) + int(with_k), *d.shape)
+    return (out[0] if with_j else torch.zeros_like(d), out[-1] if with_k else torch.zeros_like(d))
+
+
+@dataclass(frozen=True)
+class IntegralPlan:
+    """Static topology + table layout (plan.py:50-92)."""
+    topology: BasisTopology
+    atm: np.ndarray
+    bas: np.ndarray
+    env_size: int
+
+    def pack(self, parameters: BasisParameters):
+        return pack(self.topology, parameters)
+
+    def get_jk(self, parameters, density, *, screening_threshold=0.0, workers=1, with_j=True,
+               with_k=True, omega=0.0, precision="fp64", fp32_cut=DEFAULT_FP32_CUT):
+        if omega:
+            raise NotImplementedError("Range-separated (omega > 0) J/K is not built on the B200 path.")
+        atm, bas, env = self.pack(parameters)
+        d = torch.as_tensor(density)
+        if d.shape[-2:] != (self.topology.nao,) * 2:
+            raise ValueError("Density AO dimensions do not match the plan.")
+        return direct_jk(atm, bas, env, density, cart=self.topology.cart, cutoff=screening_threshold,
+                         workers=workers, with_j=with_j, with_k=with_k, precision=precision,
+                         fp32_cut=fp32_cut)
+
+
+def make_plan(topology: BasisTopology) -> IntegralPlan:
+    atm, bas, size = build_tables(topology)
+    return IntegralPlan(topology, atm, bas, size)
+
+
+@dataclass(frozen=True)
+class NativeDirectBasis:
+    """Bound (plan, parameters) J/K provider (backends/native/jk.py:70-107)."""
+    plan: IntegralPlan
+    parameters: BasisParameters
+
+    @property
+    def nao(self):
+        return self.plan.topology.nao
+
+    def get_jk(self, density, *, screening_threshold=0.0, workers=1, with_j=True, with_k=True,
+               omega=0.0, precision="fp64", fp32_cut=DEFAULT_FP32_CUT):
+        return self.plan.get_jk(self.parameters, density, screening_threshold=screening_threshold,
+                                workers=workers, with_j=with_j, with_k=with_k, omega=omega,
+                                precision=precision, fp32_cut=fp32_cut)

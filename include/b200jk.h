@@ -1,0 +1,126 @@
+/*
+ * b200jk -- B200-native (sm_100a) direct-SCF Coulomb/exchange build.
+ *
+ * Plain C ABI over raw pointers: host arrays for the libcint-layout tables,
+ * device pointers (caller-owned, stream-ordered) for densities and results.
+ * Every entry point returns 0 on success or a nonzero b200jk_status; the
+ * message of the calling thread's last failure is b200jk_last_error().
+ *
+ * Reference interfaces replaced (paths inside the reference's
+ * src/gradscf/integrals/_native/):
+ *   GradSCFDirectJK            csrc/direct_jk.cc:97-102   ("gradscf_direct_jk_cpu_v1")
+ *   GradSCFDirectJKGeometryVJPParallel
+ *                              csrc/direct_jk_geometry.cc:194-201 ("..._geometry_vjp_cpu_v2")
+ * Table layout (atm rows of 6 int32, bas rows of 8 int32, env float64) is
+ * libcint's, validated as csrc/tables.h:31-76 validates it.
+ */
+#ifndef B200JK_H
+#define B200JK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  B200JK_OK = 0,
+  B200JK_INVALID_ARGUMENT = 1, /* reference: ffi::Error::InvalidArgument */
+  B200JK_INTERNAL = 2,         /* reference: ffi::Error::Internal (CUDA failure, device status) */
+  B200JK_UNSUPPORTED = 3       /* valid input outside this build (l > 3, omega != 0) */
+} b200jk_status;
+
+/* Precision of the ERI evaluation.  J/K accumulation is FP64 in every mode. */
+typedef enum {
+  B200JK_FP64 = 0,  /* every quartet in FP64 */
+  B200JK_SPLIT = 1  /* quartets with Q_ij*Q_kl*max|D| < fp32_cut in FP32, the rest FP64 */
+} b200jk_precision;
+
+typedef struct b200jk_plan b200jk_plan;
+
+/* One molecule's libcint tables (host memory; copied during plan creation). */
+typedef struct {
+  const int32_t* atm; int32_t natm;
+  const int32_t* bas; int32_t nbas;
+  const double* env;  int32_t nenv;
+} b200jk_molecule;
+
+/* Message of this thread's last failure ("" if none). */
+const char* b200jk_last_error(void);
+
+/* Build a device-resident plan for one molecule or a batch of independent
+ * molecules: validated tables, split general contractions, primitive-pair
+ * data, Schwarz bounds Q_ij = sqrt(max |(ab|ab)|) (the reference's
+ * eri_schwarz_bounds, csrc/coulomb_shells.h:60-77) and the sorted
+ * significant-pair lists with their work items for `schwarz_cut`
+ * (quartets with Q_ij*Q_kl < schwarz_cut are skipped, as unique_eri does,
+ * csrc/coulomb_shells.h:200-212).  Rebuild when coordinates change.
+ * `device` is the CUDA ordinal the plan lives on. */
+int b200jk_plan_create(const b200jk_molecule* mols, int32_t nmol, int32_t cart,
+                       double schwarz_cut, int32_t device, b200jk_plan** out);
+void b200jk_plan_destroy(b200jk_plan* plan);
+
+/* Plan facts: output AO count of molecule `mol`, and the number of
+ * significant canonical shell quartets (i>=j, k>=l, ij>=kl, Q_ij Q_kl >= cut,
+ * counted on the reference's shells) -- the unit of the quartets/s metric. */
+int b200jk_plan_nao(const b200jk_plan* plan, int32_t mol, int32_t* nao);
+int b200jk_plan_quartets(const b200jk_plan* plan, int64_t* count);
+/* Per-molecule output block offsets into the packed density / J / K layout
+ * (molecule m occupies [offset[m], offset[m] + nao[m]^2) of each matrix). */
+int b200jk_plan_block_offsets(const b200jk_plan* plan, int64_t* offsets);
+
+/* Direct J/K (replaces GradSCFDirectJK, csrc/direct_jk.cc:7-95).
+ *   d_density : device, nb packed density sets (nb x sum_m nao_m^2, row-major
+ *               per molecule; for one molecule simply (nb, n, n)).  Need not be
+ *               symmetric unless hermi = 1 promises it.
+ *   d_out     : device, (with_j + with_k, nb, ...) like the reference's result
+ *               buffer: J first, then K; fully overwritten.
+ *   precision : B200JK_FP64 or B200JK_SPLIT (fp32_cut used only for SPLIT).
+ *   stream    : cudaStream_t (NULL = legacy default stream).
+ * Asynchronous: returns after enqueueing; a nonfinite density is reported
+ * through b200jk_check_status (or by a later synchronous call). */
+int b200jk_direct_jk(b200jk_plan* plan, const double* d_density, int32_t nb, double* d_out,
+                     int32_t with_j, int32_t with_k, int32_t hermi, int32_t precision,
+                     double fp32_cut, void* stream);
+
+/* Synchronise `stream` and turn the plan's device status word into a return
+ * code (nonfinite density -> B200JK_INVALID_ARGUMENT), clearing it. */
+int b200jk_check_status(b200jk_plan* plan, void* stream);
+
+/* One-shot drop-in with the reference handler's argument list
+ * (csrc/direct_jk.cc:7-11 + 97-102): builds a plan, runs FP64 J/K, checks the
+ * density, destroys the plan.  `workers` is accepted for ABI parity (must be
+ * >= 1) and ignored.  Synchronous. */
+int b200jk_direct_jk_tables(const int32_t* atm, int32_t natm, const int32_t* bas, int32_t nbas,
+                            const double* env, int32_t nenv, const double* d_density, int32_t nb,
+                            int32_t n, double* d_out, int32_t cart, double cutoff, int32_t workers,
+                            int32_t with_j, int32_t with_k, void* stream);
+
+/* Coordinate VJP of J/K (replaces gradscf_direct_jk_geometry_vjp_cpu_v2,
+ * csrc/direct_jk_geometry.cc:122-182): for cotangents Jbar, Kbar
+ * (d_cot: (with_j + with_k, nb, ...), same layout as d_out above) returns
+ *   g[R] = sum_abcd d(ab|cd)/dR (Jbar_ab D_cd + Kbar_ac D_bd)
+ * for every centre atom row of every molecule's atm table.
+ *   d_grad : device, (sum_m natm_m, 3), fully overwritten.
+ * Unlike the reference (which demands cutoff 0), the plan's Schwarz cut is
+ * applied; a plan built with cut 0 reproduces the reference exactly. */
+int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_t nb,
+                              const double* d_cot, int32_t with_j, int32_t with_k, double* d_grad,
+                              void* stream);
+
+/* One-electron matrices in the plan's output basis (sum_m nao_m^2 packed):
+ * which = 0 overlap, 1 kinetic, 2 nuclear attraction (atoms with nonzero
+ * charge in the atm table, point nuclei). */
+int b200jk_int1e(b200jk_plan* plan, int32_t which, double* d_out, void* stream);
+
+/* Gradient of sum_ab [ D_ab h_ab - W_ab S_ab ] with respect to every atm row
+ * (h = kinetic + nuclear attraction, including the Hellmann-Feynman operator
+ * derivative of the nuclear attraction).  d_grad: (sum_m natm_m, 3), overwritten. */
+int b200jk_int1e_grad(b200jk_plan* plan, const double* d_density, const double* d_energy_weighted,
+                      double* d_grad, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200JK_H */

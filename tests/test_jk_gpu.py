@@ -1,0 +1,154 @@
+"""GPU direct J/K (C ABI, sm_100a kernels) against the CPU oracle.
+
+Tolerances: the reference's own tests compare direct J/K with the full-ERI
+einsum at atol 2e-10 / rtol 1e-10 (tests/integrals/test_native_direct_parallel.py:60)
+and 3e-12 for H2/sto-3g (test_native_jk_dispatch.py:32); the FP64 bar of this
+build is 1e-10 max-abs against the oracle.
+"""
+import json
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not torch.cuda.is_available(), reason="needs CUDA")]
+
+import oracle  # noqa: E402
+from gradscf_b200 import jk as J  # noqa: E402
+from gradscf_b200 import _capi  # noqa: E402
+from tests.gpu_util import WATER, psd_density, tables  # noqa: E402
+
+
+def gpu_jk(atm, bas, env, d, cart, cutoff=0.0, **kw):
+    j, k = J.direct_jk(atm, bas, env, torch.as_tensor(d, device="cuda"), cart=cart, cutoff=cutoff, **kw)
+    return j.cpu().numpy(), k.cpu().numpy()
+
+
+def test_h2_sto3g_golden(golden_dir):
+    rec = json.loads((golden_dir / "h2_sto3g_jk.json").read_text())
+    top, par, sa, atm, bas, env = tables(rec["atom"], rec["basis"], True)
+    j, k = gpu_jk(atm, bas, env, np.array(rec["density"]), True)
+    np.testing.assert_allclose(j, rec["j"], atol=3e-12, rtol=3e-12)
+    np.testing.assert_allclose(k, rec["k"], atol=3e-12, rtol=3e-12)
+
+
+@pytest.mark.parametrize("cart", [False, True], ids=["sph", "cart"])
+def test_general_contraction_nonsymmetric_batch_golden(golden_dir, cart):
+    rec = json.loads((golden_dir / "h2_general_jk.json").read_text())
+    top, par, sa, atm, bas, env = tables(rec["atom"], rec["basis"], cart)
+    sub = rec["cart" if cart else "sph"]
+    j, k = gpu_jk(atm, bas, env, np.array(sub["density"]), cart)
+    np.testing.assert_allclose(j, sub["j"], atol=2e-10, rtol=1e-10)
+    np.testing.assert_allclose(k, sub["k"], atol=2e-10, rtol=1e-10)
+
+
+@pytest.mark.parametrize("basis,cart", [("cc-pvdz", False), ("6-31g*", True), ("6-31g*", False),
+                                        ("cc-pvtz", False), ("cc-pvtz", True)])
+def test_water_vs_oracle(basis, cart):
+    top, par, sa, atm, bas, env = tables(WATER, basis, cart)
+    d = psd_density(top.nao, 5, 0)
+    j0, k0 = oracle.direct_jk(atm, bas, env, d, cart=cart, workers=8)
+    j, k = gpu_jk(atm, bas, env, d, cart)
+    assert np.abs(j - j0).max() < 1e-10
+    assert np.abs(k - k0).max() < 1e-10
+
+
+def test_water_cc_pvdz_config0_screened():
+    # Config: water cc-pVDZ (24 functions), Schwarz cut 1e-12, D = C C^T seed 0.
+    top, par, sa, atm, bas, env = tables(WATER, "cc-pvdz", False)
+    assert top.nao == 24
+    d = psd_density(24, 5, 0)
+    j0, k0 = oracle.direct_jk(atm, bas, env, d, cart=False, cutoff=1e-12)
+    j, k = gpu_jk(atm, bas, env, d, False, cutoff=1e-12)
+    assert np.abs(j - j0).max() < 1e-10 and np.abs(k - k0).max() < 1e-10
+
+
+def test_water_dimer_nonsymmetric_screened():
+    atom = WATER + "; O 2.9 0.1 0.2; H 3.4 0.8 0.5; H 3.5 -0.7 0.3"
+    top, par, sa, atm, bas, env = tables(atom, "cc-pvdz", False)
+    d = np.random.default_rng(807).normal(size=(3, top.nao, top.nao)) * 0.1
+    j0, k0 = oracle.direct_jk(atm, bas, env, d, cart=False, cutoff=1e-12, workers=8)
+    j, k = gpu_jk(atm, bas, env, d, False, cutoff=1e-12)
+    assert np.abs(j - j0).max() < 1e-10 and np.abs(k - k0).max() < 1e-10
+
+
+def test_with_j_with_k_selection_and_complex():
+    top, par, sa, atm, bas, env = tables(WATER, "6-31g*", False)
+    rng = np.random.default_rng(806)
+    d = rng.normal(size=(top.nao, top.nao)) + 1j * rng.normal(size=(top.nao, top.nao))
+    j0r, k0r = oracle.direct_jk(atm, bas, env, d.real, cart=False)
+    j0i, k0i = oracle.direct_jk(atm, bas, env, d.imag, cart=False)
+    j, k = J.direct_jk(atm, bas, env, torch.as_tensor(d, device="cuda"), cart=False, with_k=False)
+    assert np.abs(j.cpu().numpy() - (j0r + 1j * j0i)).max() < 1e-10
+    assert np.count_nonzero(k.cpu().numpy()) == 0
+    j, k = J.direct_jk(atm, bas, env, torch.as_tensor(d, device="cuda"), cart=False, with_j=False)
+    assert np.abs(k.cpu().numpy() - (k0r + 1j * k0i)).max() < 1e-10
+    assert np.count_nonzero(j.cpu().numpy()) == 0
+
+
+def test_screening_linear_and_huge_cut_zero():
+    top, par, sa, atm, bas, env = tables(WATER, "cc-pvdz", False)
+    rng = np.random.default_rng(803)
+    d, t = rng.normal(size=(2, 4, top.nao, top.nao))
+    a = gpu_jk(atm, bas, env, d + 0.37 * t, False, cutoff=1e-6)
+    b = gpu_jk(atm, bas, env, d, False, cutoff=1e-6)
+    c = gpu_jk(atm, bas, env, t, False, cutoff=1e-6)
+    for x, y, z in zip(a, b, c):
+        np.testing.assert_allclose(x, y + 0.37 * z, atol=2e-10, rtol=1e-10)
+    for x in gpu_jk(atm, bas, env, d, False, cutoff=1e9):
+        assert np.count_nonzero(x) == 0
+
+
+def test_nonfinite_density_and_unsupported_inputs_raise():
+    top, par, sa, atm, bas, env = tables(WATER, "sto-3g", True)
+    d = np.full((top.nao, top.nao), np.nan)
+    with pytest.raises(ValueError, match="Nonfinite"):
+        gpu_jk(atm, bas, env, d, True)
+    top, par, sa, atm, bas, env = tables("H 0 0 0; H 0 0 1", [[4, [1.0, 1.0]]], False)
+    with pytest.raises(NotImplementedError):
+        gpu_jk(atm, bas, env, np.eye(top.nao), False)
+    bad = bas.copy(); bad[0, 2] = 0
+    with pytest.raises(ValueError, match="unsupported"):
+        J.DirectJKPlan([(atm, bad, env)], cart=False)
+
+
+def test_split_precision_error_is_small():
+    atom = WATER + "; O 2.9 0.1 0.2; H 3.4 0.8 0.5; H 3.5 -0.7 0.3"
+    top, par, sa, atm, bas, env = tables(atom, "cc-pvdz", False)
+    d = psd_density(top.nao, 10, 3)
+    plan = J.cached_plan(atm, bas, env, cart=False, cutoff=1e-12)
+    j64, k64 = plan.jk(torch.as_tensor(d, device="cuda"))
+    j32, k32 = plan.jk(torch.as_tensor(d, device="cuda"), precision="split", fp32_cut=1e-6)
+    ej = (j32 - j64).abs().max().item()
+    ek = (k32 - k64).abs().max().item()
+    assert ej < 1e-8 and ek < 1e-8
+    de = 0.5 * torch.sum(torch.as_tensor(d, device="cuda") * ((j32 - j64) - 0.5 * (k32 - k64))).item()
+    assert abs(de) < 1e-9
+
+
+def test_batched_plan_matches_single_molecule_plans():
+    mols = []
+    for shift in (0.0, 0.3):
+        atom = f"O 0 0 {shift}; H 0 0.7572 {0.5865 + shift}; H 0.1 -0.7572 {0.5865 - shift}"
+        mols.append(tables(atom, "cc-pvdz", False))
+    plan = J.DirectJKPlan([(m[3], m[4], m[5]) for m in mols], cart=False, cutoff=1e-12)
+    ds = [psd_density(m[0].nao, 5, i) for i, m in enumerate(mols)]
+    packed = torch.zeros((1, plan.packed_size), dtype=torch.float64, device="cuda")
+    for m, d in enumerate(ds):
+        packed[0, plan.offsets[m]:plan.offsets[m] + d.size] = torch.as_tensor(d.ravel(), device="cuda")
+    out = plan.jk_packed(packed, hermi=1).cpu().numpy()
+    for m, (mol, d) in enumerate(zip(mols, ds)):
+        n = mol[0].nao
+        j0, k0 = oracle.direct_jk(mol[3], mol[4], mol[5], d, cart=False, cutoff=1e-12)
+        sl = slice(plan.offsets[m], plan.offsets[m] + n * n)
+        assert np.abs(out[0, 0, sl].reshape(n, n) - j0).max() < 1e-10
+        assert np.abs(out[1, 0, sl].reshape(n, n) - k0).max() < 1e-10
+
+
+def test_quartet_count_matches_oracle():
+    atom = WATER + "; O 2.9 0.1 0.2; H 3.4 0.8 0.5; H 3.5 -0.7 0.3"
+    top, par, sa, atm, bas, env = tables(atom, "cc-pvdz", False)
+    plan = J.cached_plan(atm, bas, env, cart=False, cutoff=1e-12)
+    q = oracle.schwarz_bounds(atm, bas, env, cart=False)
+    assert plan.quartets == oracle.count_quartets(q, 1e-12)
