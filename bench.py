@@ -1,0 +1,362 @@
+"""Benchmark: direct J/K build of the (H2O)32 / cc-pVDZ cluster on B200.
+
+One step = one complete J/K build (density transform, every class-pair
+kernel, J/K finalisation) of the 768-function (H2O)32 cc-pVDZ cluster
+(seeded generator, seed 1), Schwarz cut 1e-12, one RHF-like density
+D = 2 C C^T (C ~ N(0,1)/sqrt(n), 5 occupied orbitals per water, seed 1).
+
+Headline `value`: ERI quartets/s of the split-precision build (FP32 for
+quartets with Q_ij Q_kl max|D| < 1e-6), whole job over all ranks, inputs
+resident in HBM.  Quartets = significant canonical contracted shell quartets
+of the reference's shells (i>=j, k>=l, ij>=kl, Q_ij Q_kl >= 1e-12).  The
+FP64 build is measured in the same run (`fp64` key).  L2 is flushed (512 MB
+write) before every timed step; each step is timed with CUDA events on the
+launching stream.
+
+`--impl reference` times the reference's CPU path: libcint 6.1.3 compiled
+from the reference's sources, driven by the C restatement of its direct J/K
+driver (oracle/_ref), with all host threads, one full J/K build of the
+first 8 waters of the same cluster per step.
+
+Multi-GPU (torchrun): each rank builds J/K for its own replica of the
+workload (weak scaling, no collective on the data path); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "J/K build s/iter & ERI quartets/s: split vs FP64 on B200 at |ΔE|≤1e-8 Ha"
+WORKLOAD = "(H2O)32 cc-pVDZ direct J/K (768 sph AOs), Schwarz 1e-12, seed 1"
+FP32_CUT = 1e-6
+SAMPLE_WATERS = 8
+
+
+def build_workload(nwater=32, seed=1, basis="cc-pvdz"):
+    from gradscf_b200 import basis as B, workloads as W
+    spec = W.water_cluster(nwater, seed)
+    top, par, _ = B.prepare_basis(spec, basis, cart=False)
+    atm, bas, env = B.pack(top, par)
+    c = np.random.default_rng(seed).normal(size=(top.nao, 5 * nwater)) / np.sqrt(top.nao)
+    d = 2.0 * c @ c.T
+    return top, atm, bas, env, d
+
+
+def sample_workload():
+    from gradscf_b200 import basis as B, workloads as W
+    spec = "; ".join(W.water_cluster(32, 1).split("; ")[:3 * SAMPLE_WATERS])
+    top, par, _ = B.prepare_basis(spec, "cc-pvdz", cart=False)
+    atm, bas, env = B.pack(top, par)
+    c = np.random.default_rng(1).normal(size=(top.nao, 5 * SAMPLE_WATERS)) / np.sqrt(top.nao)
+    return top, atm, bas, env, 2.0 * c @ c.T
+
+
+def cpu_reference_run(steps, warmup):
+    """Time the reference CPU path on the bounded sample; returns (q/s, cores, sample)."""
+    import oracle
+    top, atm, bas, env, d = sample_workload()
+    q = oracle.count_quartets(oracle.schwarz_bounds(atm, bas, env, cart=False), 1e-12)
+    cores = os.cpu_count() or 1
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        oracle.direct_jk(atm, bas, env, d, cart=False, cutoff=1e-12, workers=cores)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    sample = (f"one full J/K build of the first {SAMPLE_WATERS} waters of the seed-1 (H2O)32 "
+              f"cluster ({top.nao} sph AOs, {q} significant quartets), cc-pVDZ, Schwarz 1e-12, "
+              f"workers={cores}")
+    return q / float(np.mean(times)), cores, sample, float(np.mean(times))
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) != 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[2:]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--nwater", type=int, default=32,
+                    help="cluster size (profiling runs use a smaller case; the benchmark is 32)")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU baseline leg (profiling runs)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        value, cores, sample, step_s = cpu_reference_run(args.steps, args.warmup)
+        line = {"metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": WORKLOAD, "sample": sample},
+                "cpu_baseline": {"value": value, "unit": "quartets/s", "cores": cores,
+                                 "kind": "reference", "sample": sample},
+                "e2e": {"value": value, "unit": "quartets/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    from gradscf_b200 import _capi, flop_model
+    from gradscf_b200.jk import DirectJKPlan
+    import ctypes
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    lib = _capi.lib()
+
+    top, atm, bas, env, dnp = build_workload(args.nwater)
+    plan = DirectJKPlan([(atm, bas, env)], cart=False, cutoff=1e-12, device=dev)
+    n = top.nao
+    d = torch.as_tensor(dnp.reshape(1, n * n), device=dev)
+    out = torch.empty((2, 1, n * n), dtype=torch.float64, device=dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    peaks = {}
+    for name, flag in (("fp64", 1), ("fp32", 0)):
+        v = ctypes.c_double()
+        _capi.check(lib.b200jk_measure_fma_peak(flag, ctypes.byref(v), ctypes.c_void_p(stream.cuda_stream)))
+        peaks[name] = v.value
+
+    def step(precision):
+        plan.jk_packed(d, hermi=1, precision=precision, fp32_cut=FP32_CUT, out=out, check=False)
+
+    for _ in range(args.warmup):
+        step("fp64")
+        step("split")
+    _capi.check(lib.b200jk_check_status(plan._h, ctypes.c_void_p(stream.cuda_stream)))
+    torch.cuda.synchronize()
+
+    def energy(o):
+        j = o[0, 0].reshape(n, n)
+        k = o[1, 0].reshape(n, n)
+        dd = d[0].reshape(n, n)
+        return (0.5 * torch.sum(dd * j) - 0.25 * torch.sum(dd * k)).item()
+
+    step("fp64")
+    ref_out = out.clone()
+    e64 = energy(ref_out)
+    step("split")
+    e32 = energy(out)
+    max_dj = (out[0] - ref_out[0]).abs().max().item()
+    max_dk = (out[1] - ref_out[1]).abs().max().item()
+
+    nc = _capi.NCLASS
+    q = (ctypes.c_int64 * nc)(); pq = (ctypes.c_int64 * nc)()
+    _capi.check(lib.b200jk_plan_class_stats(plan._h, q, pq))
+    q64 = (ctypes.c_int64 * nc)(); q32 = (ctypes.c_int64 * nc)()
+    pq64 = (ctypes.c_int64 * nc)(); pq32 = (ctypes.c_int64 * nc)()
+    _capi.check(lib.b200jk_plan_split_stats(plan._h, ctypes.c_void_p(stream.cuda_stream), q64, q32, pq64, pq32))
+    nclasspairs = sum(1 for c in range(nc) if q[c] > 0)
+
+    results = {}
+    clocks = ClockSampler(local)
+    with clocks:
+        for precision in ("fp64", "split"):
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            lib.b200jk_plan_set_profiling(plan._h, 1)
+            times = []
+            for _ in range(args.steps):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                step(precision)
+                e1.record(stream)
+                times.append((e0, e1))
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            lib.b200jk_plan_set_profiling(plan._h, 0)
+            ms = [a.elapsed_time(b) for a, b in times]
+            ms64 = (ctypes.c_double * nc)(); ms32 = (ctypes.c_double * nc)(); nl = (ctypes.c_int32 * nc)()
+            _capi.check(lib.b200jk_plan_profile(plan._h, ms64, ms32, nl))
+            step_ms = float(np.mean(ms))
+            if dist:
+                t = torch.tensor([step_ms], device=dev)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                step_ms = t.item()
+            results[precision] = {"ms": step_ms, "ms64": list(ms64), "ms32": list(ms32),
+                                  "launches": list(nl)}
+        # end-to-end through the public API with pinned host buffers
+        hd = torch.empty((1, n * n), dtype=torch.float64, pin_memory=True)
+        hd.copy_(d.cpu())
+        hout = torch.empty((2, 1, n * n), dtype=torch.float64, pin_memory=True)
+        dd = torch.empty_like(d)
+        e2e_ms = []
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            dd.copy_(hd, non_blocking=True)
+            plan.jk_packed(dd, hermi=1, precision="split", fp32_cut=FP32_CUT, out=out, check=False)
+            hout.copy_(out, non_blocking=True)
+            e1.record(stream)
+            e2e_ms.append((e0, e1))
+        torch.cuda.synchronize()
+        e2e_step = float(np.mean([a.elapsed_time(b) for a, b in e2e_ms]))
+        if dist:
+            t = torch.tensor([e2e_step], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_step = t.item()
+
+    quartets = plan.quartets
+    qps = {p: world * quartets / (results[p]["ms"] * 1e-3) for p in results}
+
+    # roofline of the dominant kernel of the split step
+    classes = _capi.QUARTET_CLASSES
+    best = None
+    for c in range(nc):
+        for kind, msk, pqk, qk, peak in (("fp64", "ms64", pq64, q64, peaks["fp64"]),
+                                         ("fp32", "ms32", pq32, q32, peaks["fp32"])):
+            t = results["split"][msk][c]
+            if t > 0 and (best is None or t > best[0]):
+                flops = flop_model.class_flops(classes[c], pqk[c], qk[c])
+                best = (t, c, kind, flops, peak)
+    t_ms, c, kind, flops, peak = best
+    launches = results["split"]["launches"][c] / 2 / args.steps  # fp64+fp32 share the count
+    per_launch_ms = t_ms / args.steps
+    achieved = flops / (per_launch_ms * 1e-3) / 1e12
+    total_ms = sum(results["split"]["ms64"]) + sum(results["split"]["ms32"])
+    roofline = {"bound": kind, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None,
+                "kernel": f"class ({classes[c][0]}{classes[c][1]}|{classes[c][2]}{classes[c][3]}) {kind}",
+                "share_of_step": t_ms / total_ms,
+                "peak_source": f"measured {kind} FMA microkernel on this GPU (b200jk_measure_fma_peak)"}
+    # whole-build FLOP rate in FP64 mode (all classes)
+    fl64 = sum(flop_model.class_flops(classes[c], pq[c], q[c]) for c in range(nc))
+    fp64_build = {"ms_per_build": results["fp64"]["ms"], "quartets_per_s": qps["fp64"],
+                  "model_tflops": fl64 / (results["fp64"]["ms"] * 1e-3) / 1e12,
+                  "frac_of_fp64_peak": fl64 / (results["fp64"]["ms"] * 1e-3) / 1e12 / peaks["fp64"]}
+
+    top = []
+    for c in range(nc):
+        for kind, msk, pqk, qk in (("fp64", "ms64", pq64, q64), ("fp32", "ms32", pq32, q32)):
+            t = results["split"][msk][c] / args.steps
+            if t > 0:
+                fl = flop_model.class_flops(classes[c], pqk[c], qk[c])
+                top.append({"class": "(%d%d|%d%d)" % classes[c], "prec": kind, "ms": round(t, 3),
+                            "quartets": int(qk[c]), "prim_quartets": int(pqk[c]),
+                            "tflops": round(fl / (t * 1e-3) / 1e12, 3)})
+    top.sort(key=lambda r: -r["ms"])
+    gpu_launches = args.steps * (2 + 1 + nclasspairs + 2 * nclasspairs)
+    line = {"metric": METRIC, "value": qps["split"], "unit": "quartets/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": results["split"]["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64 split (f64 accumulation)", "data": "synthetic",
+            "config": {"workload": WORKLOAD if args.nwater == 32 else f"(H2O){args.nwater} cc-pVDZ (profiling case)",
+                       "quartets": quartets, "nao": n,
+                       "fp32_cut": FP32_CUT, "density": "2 C C^T, C~N(0,1)/sqrt(n), 160 occ, seed 1",
+                       "l2": "flushed (512 MB write) before every timed step",
+                       "parallelism": f"replicas x{world}"},
+            "fp64": fp64_build,
+            "split_speedup_vs_fp64": results["fp64"]["ms"] / results["split"]["ms"],
+            "split_error": {"max_abs_dJ": max_dj, "max_abs_dK": max_dk,
+                            "dE_2e_hartree": abs(e32 - e64)},
+            "split_fraction_fp32_quartets": sum(q32) / max(1, sum(q32) + sum(q64)),
+            "e2e": {"value": world * quartets / (e2e_step * 1e-3), "unit": "quartets/s",
+                    "ms_per_step": e2e_step, "h2d_bytes_per_step": int(d.numel() * 8),
+                    "d2h_bytes_per_step": int(out.numel() * 8)},
+            "roofline": roofline, "gpu_launches": gpu_launches, "clocks": clocks.summary(),
+            "top_kernels_split_step": top[:8]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        value, cores, sample, _ = cpu_reference_run(1, 0)
+        line["cpu_baseline"] = {"value": value, "unit": "quartets/s", "cores": cores,
+                                "kind": "reference", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line))
+    plan.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

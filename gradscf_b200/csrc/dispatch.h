@@ -5,7 +5,6 @@
 namespace b200jk {
 
 struct JKArgs;
-struct GradArgs;
 
 constexpr int kMaxL = 3;
 constexpr int kPairClasses = (kMaxL + 1) * (kMaxL + 2) / 2;              // 10
@@ -13,7 +12,7 @@ constexpr int kQuartetClasses = kPairClasses * (kPairClasses + 1) / 2;   // 55
 
 using JKLauncher = int (*)(const JKArgs&, cudaStream_t);
 using SchwarzLauncher = int (*)(const JKArgs&, int npairs, int cart, cudaStream_t);
-using GradLauncher = int (*)(const GradArgs&, cudaStream_t);
+using GradLauncher = int (*)(const JKArgs&, cudaStream_t);
 
 struct DispatchTable {
   JKLauncher jk64[kQuartetClasses] = {};
@@ -86,7 +85,6 @@ inline int quartet_class(int x, int y) { return x * (x + 1) / 2 + y; }      // x
 #define B200JK_DECLARE_REG(x, y) void register_jk_class_##x##_##y(DispatchTable&);
 B200JK_FOR_EACH_CLASS_PAIR(B200JK_DECLARE_REG)
 #undef B200JK_DECLARE_REG
-void register_grad_classes(DispatchTable&);
 
 const DispatchTable& dispatch();
 

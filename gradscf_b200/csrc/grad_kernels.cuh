@@ -1,0 +1,162 @@
+// Coordinate VJP of J/K: sum over canonical screened quartets of
+//   dE = sum_abcd d(ab|cd)/dR * Gamma_abcd,
+// Gamma = the eight-permutation symmetrisation (times the degeneracy scale
+// s of load_quartet) of  Jbar_ab D_cd + Kbar_ac D_bd  (the reference's
+// transposed contraction, csrc/direct_jk_geometry.cc:68-84, which runs over
+// all n^4 entries instead).  Derivatives recomputed, never stored:
+//   d/dA_x phi_a = 2 alpha phi_{a+1x} - a_x phi_{a-1x}  (same for B, C),
+//   d/dD = -(d/dA + d/dB + d/dC)  (translational invariance).
+// Team layout as the J/K team path: 2D integrals with raised bra/ket
+// indices in shared memory, each lane owns a strided slice of the Cartesian
+// block, nine gradient partials per lane reduced across the team.
+#pragma once
+#include "jk_kernels.cuh"
+
+namespace b200jk {
+
+template <int LA, int LB, int LC, int LD, int TEAM>
+struct GradCfg {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  static constexpr int NROOT = (CI::L + 1) / 2 + 1;
+  static constexpr int NG = (LA + 2) * (LB + 2) * (LC + 2) * (LD + 1);
+  static constexpr int NK = (CI::NOUT + TEAM - 1) / TEAM;
+  static constexpr int ELEMS = 3 * NROOT * NG + 2 * NROOT;
+  static constexpr size_t bytes() { return (size_t)ELEMS * 8; }
+  __host__ __device__ static constexpr int idx(int a, int b, int c, int d) {
+    return ((a * (LB + 2) + b) * (LC + 2) + c) * (LD + 1) + d;
+  }
+};
+
+// Raw Cartesian Gamma of one AO quartet (a, b, c, d), summed over batches.
+__device__ __forceinline__ double gamma_abcd(const JKArgs& args, long long base, int n, int a, int b,
+                                             int c, int d) {
+  double gsum = 0.0;
+  for (int e = 0; e < args.gnb; ++e) {
+    const double* D = args.dens + e * args.dstride + base;
+    const double* J = args.cot_j ? args.cot_j + e * args.dstride + base : nullptr;
+    const double* K = args.cot_k ? args.cot_k + e * args.dstride + base : nullptr;
+#define M_(X, i, j) X[(long long)(i) * n + (j)]
+    if (J)
+      gsum += (M_(J, a, b) + M_(J, b, a)) * (M_(D, c, d) + M_(D, d, c)) +
+              (M_(J, c, d) + M_(J, d, c)) * (M_(D, a, b) + M_(D, b, a));
+    if (K)
+      gsum += M_(K, a, c) * M_(D, b, d) + M_(K, c, a) * M_(D, d, b) + M_(K, b, c) * M_(D, a, d) +
+              M_(K, c, b) * M_(D, d, a) + M_(K, a, d) * M_(D, b, c) + M_(K, d, a) * M_(D, c, b) +
+              M_(K, b, d) * M_(D, a, c) + M_(K, d, b) * M_(D, c, a);
+#undef M_
+  }
+  return gsum;
+}
+
+template <int LA, int LB, int LC, int LD, int TEAM>
+__global__ void grad_team_kernel(JKArgs args) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using GC = GradCfg<LA, LB, LC, LD, TEAM>;
+  constexpr int N = GC::NROOT;
+  constexpr int NG = GC::NG;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x % TEAM;
+  const int team = threadIdx.x / TEAM;
+  const int nteams = blockDim.x / TEAM;
+  const unsigned mask =
+      TEAM == 32 ? 0xffffffffu : (((1u << TEAM) - 1u) << ((threadIdx.x % 32) / TEAM * TEAM));
+  double* G = reinterpret_cast<double*>(smem_raw) + (size_t)team * GC::ELEMS;
+  double* roots = G + 3 * N * NG;
+  const int4 w = args.work[blockIdx.x];
+  const int bra = args.bra_pairs[w.x];
+  for (int k = w.y + team; k < w.z; k += nteams) {
+    QuartetGeom g;
+    load_quartet(args, bra, args.ket_pairs[k], g);
+    const long long base = args.mol_base[g.mol];
+    const int n = args.mol_n[g.mol];
+    double gam[GC::NK];
+    int exps[GC::NK];   // packed exponent digits of (a, b, c, d) per axis
+#pragma unroll
+    for (int q = 0; q < GC::NK; ++q) {
+      const int o = lane + q * TEAM;
+      gam[q] = 0.0;
+      exps[q] = -1;
+      if (o < CI::NOUT) {
+        const int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
+        const int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
+        gam[q] = g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id);
+        exps[q] = ia | (ib << 4) | (ic << 8) | (id << 12);
+      }
+    }
+    double dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
+    for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
+      const double4 P = args.pp_data[i];
+      const double2 PA = args.pp_aux[i];
+      const double alpha = args.pp_exp[i].x, beta = args.pp_exp[i].y;
+      for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
+        PrimQ<double> s;
+        prim_setup<double>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
+        const double gamma_c = args.pp_exp[j].x;
+        for (int f = lane; f < 2 * N; f += TEAM) roots[f] = rys_one<N, double>(s.t, f, args.tb);
+        __syncwarp(mask);
+        for (int tsk = lane; tsk < 3 * N; tsk += TEAM) {
+          const int r = tsk / 3, ax = tsk - 3 * r;
+          RootCoef<double> rc;
+          root_coef<double>(s, roots[r], rc);
+          const double abd = ax == 0 ? g.abx : (ax == 1 ? g.aby : g.abz);
+          const double cdd = ax == 0 ? g.cdx : (ax == 1 ? g.cdy : g.cdz);
+          const double g00 = ax == 2 ? roots[N + r] * s.pref : 1.0;
+          build_g<LA + 1, LB + 1, LC + 1, LD, double>(rc.c00[ax], rc.c0p[ax], rc.b10, rc.b01, rc.b00, g00,
+                                                      abd, cdd, G + (r * 3 + ax) * NG);
+        }
+        __syncwarp(mask);
+#pragma unroll
+        for (int q = 0; q < GC::NK; ++q) {
+          if (exps[q] < 0 || gam[q] == 0.0) continue;
+          const int ia = exps[q] & 15, ib = (exps[q] >> 4) & 15, ic = (exps[q] >> 8) & 15, id = exps[q] >> 12;
+          const int la[3] = {cart_lx(LA, ia), cart_ly(LA, ia), cart_lz(LA, ia)};
+          const int lb[3] = {cart_lx(LB, ib), cart_ly(LB, ib), cart_lz(LB, ib)};
+          const int lc[3] = {cart_lx(LC, ic), cart_ly(LC, ic), cart_lz(LC, ic)};
+          const int ld[3] = {cart_lx(LD, id), cart_ly(LD, id), cart_lz(LD, id)};
+          for (int r = 0; r < N; ++r) {
+            double v[3], fa[3], fb[3], fc[3];
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+              const double* Gx = G + (r * 3 + x) * NG;
+              const int a = la[x], b = lb[x], c = lc[x], d = ld[x];
+              v[x] = Gx[GC::idx(a, b, c, d)];
+              fa[x] = 2.0 * alpha * Gx[GC::idx(a + 1, b, c, d)] - (a ? a * Gx[GC::idx(a - 1, b, c, d)] : 0.0);
+              fb[x] = 2.0 * beta * Gx[GC::idx(a, b + 1, c, d)] - (b ? b * Gx[GC::idx(a, b - 1, c, d)] : 0.0);
+              fc[x] = 2.0 * gamma_c * Gx[GC::idx(a, b, c + 1, d)] - (c ? c * Gx[GC::idx(a, b, c - 1, d)] : 0.0);
+            }
+            const double gq = gam[q];
+            const double yz = v[1] * v[2], xz = v[0] * v[2], xy = v[0] * v[1];
+            dA[0] += gq * fa[0] * yz; dA[1] += gq * fa[1] * xz; dA[2] += gq * fa[2] * xy;
+            dB[0] += gq * fb[0] * yz; dB[1] += gq * fb[1] * xz; dB[2] += gq * fb[2] * xy;
+            dC[0] += gq * fc[0] * yz; dC[1] += gq * fc[1] * xz; dC[2] += gq * fc[2] * xy;
+          }
+        }
+        __syncwarp(mask);
+      }
+    }
+    // reduce the nine partials over the team; lane 0 adds to the four centres
+#pragma unroll
+    for (int x = 0; x < 3; ++x)
+#pragma unroll
+      for (int off = TEAM / 2; off > 0; off >>= 1) {
+        dA[x] += __shfl_down_sync(mask, dA[x], off, TEAM);
+        dB[x] += __shfl_down_sync(mask, dB[x], off, TEAM);
+        dC[x] += __shfl_down_sync(mask, dC[x], off, TEAM);
+      }
+    if (lane == 0) {
+      double* gA = args.grad + 3LL * args.ws_atm[g.A];
+      double* gB = args.grad + 3LL * args.ws_atm[g.B];
+      double* gC = args.grad + 3LL * args.ws_atm[g.C];
+      double* gD = args.grad + 3LL * args.ws_atm[g.D];
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        atomicAdd(gA + x, dA[x]);
+        atomicAdd(gB + x, dB[x]);
+        atomicAdd(gC + x, dC[x]);
+        atomicAdd(gD + x, -(dA[x] + dB[x] + dC[x]));
+      }
+    }
+  }
+}
+
+}  // namespace b200jk

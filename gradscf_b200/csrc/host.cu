@@ -44,7 +44,6 @@ const DispatchTable& dispatch() {
 #define B200JK_CALL_REG(x, y) register_jk_class_##x##_##y(table);
     B200JK_FOR_EACH_CLASS_PAIR(B200JK_CALL_REG)
 #undef B200JK_CALL_REG
-    register_grad_classes(table);
   });
   return table;
 }
@@ -243,6 +242,72 @@ __global__ void jk_out_kernel(const double* __restrict__ vj, const double* __res
   if (with_k) out[(long long)((with_j ? nb : 0) + e) * out_stride + o] = kv;
 }
 
+// Output-basis matrices -> raw Cartesian, X_raw = T X T^T (no symmetrisation).
+__global__ void mat_in_kernel(const double* __restrict__ xin, double* __restrict__ xout,
+                              long long out_stride, long long cart_stride,
+                              const long long* mol_out_base, const int* mol_nout,
+                              const long long* mol_cart_base, const int* mol_ncart,
+                              const int* cart_ws, const int4* ws_info, const int* mol_cart_ao,
+                              const double* c2s) {
+  const int mol = blockIdx.y;
+  const int e = blockIdx.z;
+  const int nc = mol_ncart[mol];
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)nc * nc) return;
+  const int i = (int)(idx / nc), j = (int)(idx % nc);
+  const int no = mol_nout[mol];
+  const int wi = cart_ws[mol_cart_ao[mol] + i], wj = cart_ws[mol_cart_ao[mol] + j];
+  const int4 si = ws_info[wi], sj = ws_info[wj];
+  const double* ti = c2s + si.y * kTS + (i - si.x) * kTW;
+  const double* tj = c2s + sj.y * kTS + (j - sj.x) * kTW;
+  const double* x = xin + (long long)e * out_stride + mol_out_base[mol];
+  double v = 0.0;
+  for (int fa = 0; fa < kTW; ++fa) {
+    if (ti[fa] == 0.0) continue;
+    for (int fb = 0; fb < kTW; ++fb)
+      if (tj[fb] != 0.0) v += ti[fa] * tj[fb] * x[(long long)(si.w + fa) * no + sj.w + fb];
+  }
+  xout[(long long)e * cart_stride + mol_cart_base[mol] + (long long)i * nc + j] = v;
+}
+
+// Raw Cartesian matrix -> output basis, M_out = T^T M T (no symmetrisation).
+__global__ void cart_to_out_kernel(const double* __restrict__ m, double* __restrict__ out,
+                                   const long long* mol_out_base, const int* mol_nout,
+                                   const long long* mol_cart_base, const int* mol_ncart,
+                                   const int* out_ws, const int4* ws_info, const int* mol_out_ao,
+                                   const double* c2s) {
+  const int mol = blockIdx.y;
+  const int no = mol_nout[mol];
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)no * no) return;
+  const int a = (int)(idx / no), b = (int)(idx % no);
+  const int wa = out_ws[mol_out_ao[mol] + a], wb = out_ws[mol_out_ao[mol] + b];
+  const int4 sa = ws_info[wa], sb = ws_info[wb];
+  const int fa = a - sa.w, fb = b - sb.w;
+  const int na = (sa.y + 1) * (sa.y + 2) / 2, nbf = (sb.y + 1) * (sb.y + 2) / 2;
+  const double* ta = c2s + sa.y * kTS;
+  const double* tb = c2s + sb.y * kTS;
+  const int nc = mol_ncart[mol];
+  const long long cb = mol_cart_base[mol];
+  double v = 0.0;
+  for (int i = 0; i < na; ++i) {
+    const double x = ta[i * kTW + fa];
+    if (x == 0.0) continue;
+    for (int j = 0; j < nbf; ++j) {
+      const double y = tb[j * kTW + fb];
+      if (y == 0.0) continue;
+      v += x * y * m[cb + (long long)(sa.x + i) * nc + sb.x + j];
+    }
+  }
+  out[mol_out_base[mol] + (long long)a * no + b] = v;
+}
+
+__global__ void to_float_kernel(const double* __restrict__ x, float* __restrict__ y, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = float(x[i]);
+}
+
 __global__ void maxabs_kernel(const double* __restrict__ x, long long n, double* out) {
   double m = 0.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -255,23 +320,22 @@ __global__ void maxabs_kernel(const double* __restrict__ x, long long n, double*
     atomicMax(reinterpret_cast<unsigned long long*>(out), (unsigned long long)__double_as_longlong(m));
 }
 
-// First ket position (within the bra's ket range) computed in FP32:
-// Q_bra * Q_ket * max|D| < fp32_cut.  Ket bounds are sorted descending.
-__global__ void split_kernel(const int2* __restrict__ bra_kets, const double* __restrict__ bra_q,
+// Per work item: first ket position of its range computed in FP32,
+// Q_bra * Q_ket * max|D| < fp32_cut (ket bounds sorted descending).
+__global__ void split_kernel(const int4* __restrict__ work, const double* __restrict__ bra_q,
                              const double* __restrict__ ket_q, const double* maxd, double fp32_cut,
-                             int nbra, int* __restrict__ split) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nbra) return;
-  const int2 r = bra_kets[b];
-  const double f = bra_q[b] * (*maxd);
-  int lo = r.x, hi = r.y;
-  // invariant: kets < lo are FP64, kets >= hi are FP32
+                             int nwork, int* __restrict__ split) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nwork) return;
+  const int4 w = work[i];
+  const double f = bra_q[w.x] * (*maxd);
+  int lo = w.y, hi = w.z;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
     if (ket_q[mid] * f < fp32_cut) hi = mid;
     else lo = mid + 1;
   }
-  split[b] = lo;
+  split[i] = lo;
 }
 
 // ---------------------------------------------------------------- plan creation
@@ -319,7 +383,9 @@ static JKArgs base_args(const Plan& p) {
   a.sh_xyz = p.d_ws_xyz.as<double4>();
   a.pair_info = p.d_pair_info.as<int4>();
   a.pp_data = p.d_pp_data.as<double4>();
-  a.pp_k = p.d_pp_k.as<double>();
+  a.pp_aux = p.d_pp_aux.as<double2>();
+  a.pp_exp = p.d_pp_exp.as<double2>();
+  a.ws_atm = p.d_ws_atm.as<int>();
   a.mol_base = p.d_mol_base_cart.as<long long>();
   a.mol_n = p.d_mol_ncart.as<int>();
   a.tb = plan_tables(p);
@@ -389,7 +455,7 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
   p.cart_stride = cb;
   // ---- shell pairs and primitive pairs
   std::vector<double4> pp_data;
-  std::vector<double> pp_k;
+  std::vector<double2> pp_aux, pp_exp;
   int ws0 = 0;
   for (int m = 0; m < nmol; ++m) {
     int wsn = ws0;
@@ -411,7 +477,8 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
             if (expo > 40.0 || ca == 0.0 || cbv == 0.0) continue;  // exp(-40) ~ 4e-18
             pp_data.push_back(make_double4((a * ra.x + b * rb.x) / pe, (a * ra.y + b * rb.y) / pe,
                                            (a * ra.z + b * rb.z) / pe, pe));
-            pp_k.push_back(std::exp(-expo) * ca * cbv);
+            pp_aux.push_back(make_double2(std::exp(-expo) * ca * cbv / pe, 0.5 / pe));
+            pp_exp.push_back(make_double2(a, b));
           }
         const int cnt = (int)pp_data.size() - off;
         if (cnt == 0) continue;
@@ -426,7 +493,8 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
   upload(p.d_ws_xyz, p.ws_xyz.data(), p.ws_xyz.size() * sizeof(double4));
   upload(p.d_pair_info, p.pair_info.data(), p.pair_info.size() * sizeof(int4));
   upload(p.d_pp_data, pp_data.data(), pp_data.size() * sizeof(double4));
-  upload(p.d_pp_k, pp_k.data(), pp_k.size() * sizeof(double));
+  upload(p.d_pp_aux, pp_aux.data(), pp_aux.size() * sizeof(double2));
+  upload(p.d_pp_exp, pp_exp.data(), pp_exp.size() * sizeof(double2));
   upload(p.d_mol_base_cart, p.mol_cart_base.data(), nmol * sizeof(long long));
   upload(p.d_mol_ncart, p.mol_ncart.data(), nmol * sizeof(int));
   upload(p.d_mol_base_out, p.mol_out_base.data(), nmol * sizeof(long long));
@@ -447,7 +515,11 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     std::vector<double2> ec(p.ws_exp.size());
     for (size_t i = 0; i < ec.size(); ++i) ec[i] = make_double2(p.ws_exp[i], p.ws_coef[i]);
     upload(p.d_ws_prim, ec.data(), ec.size() * sizeof(double2));
-    upload(p.d_ws_prim_off, p.ws_prim_off.data(), p.ws_prim_off.size() * sizeof(int));
+    std::vector<int> off = p.ws_prim_off;
+    off.push_back((int)p.ws_exp.size());
+    upload(p.d_ws_prim_off, off.data(), off.size() * sizeof(int));
+    upload(p.d_mol_atm, p.mol_atm_off.data(), nmol * sizeof(int));
+    upload(p.d_mol_natm, p.mol_natm.data(), nmol * sizeof(int));
   }
   CUDA_OK(p.d_status.ensure(sizeof(int)));
   CUDA_OK(cudaMemset(p.d_status.ptr, 0, sizeof(int)));
@@ -455,6 +527,22 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
   // ---- Schwarz bounds on the device, one launch per pair class
   std::vector<std::vector<int>> by_class(kPairClasses);
   for (int q = 0; q < p.npair; ++q) by_class[p.pair_class[q]].push_back(q);
+  for (int c = 0; c < kPairClasses; ++c) {
+    p.n_all_pairs[c] = (int)by_class[c].size();
+    if (p.n_all_pairs[c]) upload(p.d_all_pairs[c], by_class[c].data(), by_class[c].size() * sizeof(int));
+  }
+  // molecule AO starts (global Cartesian / output AO index) for the transforms
+  {
+    std::vector<int> v(2 * nmol);
+    int c = 0, o = 0;
+    for (int m = 0; m < nmol; ++m) {
+      v[m] = c;
+      v[nmol + m] = o;
+      c += p.mol_ncart[m];
+      o += p.mol_nout[m];
+    }
+    upload(p.d_mol_ao_off, v.data(), v.size() * sizeof(int));
+  }
   CUDA_OK(p.d_q_work.ensure(std::max(p.npair, 1) * sizeof(double)));
   {
     std::vector<DevBuf> lists(kPairClasses);
@@ -500,18 +588,33 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
       if (cut > 0 && p.pair_q[q] * qmax_mol[m] < cut) continue;  // coulomb_shells.h:203
       ids.push_back(q);
     }
+    // Order: molecule, then primitive-pair count (so a warp's kets share
+    // their contraction length), then Q descending (screening prefix).
     std::sort(ids.begin(), ids.end(), [&](int a, int b) {
       const int ma = p.ws_info[p.pair_info[a].x].z, mb = p.ws_info[p.pair_info[b].x].z;
       if (ma != mb) return ma < mb;
+      if (p.pair_info[a].w != p.pair_info[b].w) return p.pair_info[a].w < p.pair_info[b].w;
       if (p.pair_q[a] != p.pair_q[b]) return p.pair_q[a] > p.pair_q[b];
       return a < b;
     });
     L.pairs = ids;
     L.q.resize(ids.size());
     for (size_t i = 0; i < ids.size(); ++i) L.q[i] = p.pair_q[ids[i]];
+    L.npp_prefix.assign(ids.size() + 1, 0);
+    for (size_t i = 0; i < ids.size(); ++i) L.npp_prefix[i + 1] = L.npp_prefix[i] + p.pair_info[ids[i]].w;
     L.mol_begin.assign(nmol + 1, 0);
     for (int q : ids) L.mol_begin[p.ws_info[p.pair_info[q].x].z + 1]++;
     for (int m = 0; m < nmol; ++m) L.mol_begin[m + 1] += L.mol_begin[m];
+    L.segs.assign(nmol, {});
+    for (size_t i = 0; i < ids.size();) {
+      size_t j = i + 1;
+      const int m = p.ws_info[p.pair_info[ids[i]].x].z;
+      while (j < ids.size() && p.ws_info[p.pair_info[ids[j]].x].z == m &&
+             p.pair_info[ids[j]].w == p.pair_info[ids[i]].w)
+        ++j;
+      L.segs[m].push_back(make_int2((int)i, (int)j));
+      i = j;
+    }
     upload(L.d_pairs, ids.data(), ids.size() * sizeof(int));
     upload(L.d_q, L.q.data(), L.q.size() * sizeof(double));
   }
@@ -529,32 +632,35 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
       W->y = y;
       W->nbra = (int)X.pairs.size();
       std::vector<int4> items;
-      std::vector<int2> bk(W->nbra);
       for (int bp = 0; bp < W->nbra; ++bp) {
         const int m = p.ws_info[p.pair_info[X.pairs[bp]].x].z;
-        const int lo = Y.mol_begin[m], hi0 = Y.mol_begin[m + 1];
-        int hi = hi0;
-        if (cut > 0) {
-          const double qb = X.q[bp];
-          int a = lo, b = hi0;  // first ket with qb*qk < cut
-          while (a < b) {
-            const int mid = (a + b) >> 1;
-            if (qb * Y.q[mid] < cut) b = mid;
-            else a = mid + 1;
+        const double qb = X.q[bp];
+        const long long npa = p.pair_info[X.pairs[bp]].w;
+        for (const int2 seg : Y.segs[m]) {
+          const int lo = seg.x;
+          if (x == y && lo > bp) break;  // canonical: ket position <= bra position
+          int hi = seg.y;
+          if (cut > 0) {
+            int a = lo, b = seg.y;  // first ket with qb*qk < cut (bounds sorted descending)
+            while (a < b) {
+              const int mid = (a + b) >> 1;
+              if (qb * Y.q[mid] < cut) b = mid;
+              else a = mid + 1;
+            }
+            hi = a;
           }
-          hi = a;
+          if (x == y) hi = std::min(hi, bp + 1);
+          if (hi <= lo) continue;
+          W->quartets += hi - lo;
+          W->prim_quartets += npa * (Y.npp_prefix[hi] - Y.npp_prefix[lo]);
+          for (int s = lo; s < hi; s += chunk) items.push_back(make_int4(bp, s, std::min(hi, s + chunk), 0));
         }
-        if (x == y) hi = std::min(hi, bp + 1);
-        if (hi < lo) hi = lo;
-        bk[bp] = make_int2(lo, hi);
-        W->quartets += hi - lo;
-        for (int s = lo; s < hi; s += chunk) items.push_back(make_int4(bp, s, std::min(hi, s + chunk), 0));
       }
       W->nwork = (int)items.size();
       if (W->nwork == 0) { delete W; continue; }
       upload(W->work, items.data(), items.size() * sizeof(int4));
-      upload(W->bra_kets, bk.data(), bk.size() * sizeof(int2));
-      CUDA_OK(W->split.ensure(W->nbra * sizeof(int)));
+      W->h_items = items;
+      CUDA_OK(W->split.ensure(W->nwork * sizeof(int)));
       p.work.push_back(W);
     }
   // ---- quartet count on the reference's shells (parent pairs, canonical)
@@ -589,12 +695,34 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
   return plan.release();
 }
 
+}  // namespace b200jk
+#include "one_electron.h"
+namespace b200jk {
+
+static OneArgs one_args(const Plan& p) {
+  OneArgs a{};
+  a.pair_info = p.d_pair_info.as<int4>();
+  a.ws_info = p.d_ws_info.as<int4>();
+  a.ws_xyz = p.d_ws_xyz.as<double4>();
+  a.prim = p.d_ws_prim.as<double2>();
+  a.prim_off = p.d_ws_prim_off.as<int>();
+  a.atoms = p.d_atoms.as<double4>();
+  a.mol_atm_off = p.d_mol_atm.as<int>();
+  a.mol_natm = p.d_mol_natm.as<int>();
+  a.mol_base = p.d_mol_base_cart.as<long long>();
+  a.mol_n = p.d_mol_ncart.as<int>();
+  a.ws_atm = p.d_ws_atm.as<int>();
+  a.tb = plan_tables(p);
+  return a;
+}
+
 // ---------------------------------------------------------------- J/K execution
 static void ensure_scratch(Plan& p, int nb) {
   if (p.scratch_nb >= nb) return;
   CUDA_OK(p.d_dens.ensure((size_t)2 * nb * p.cart_stride * sizeof(double)));
   CUDA_OK(p.d_vj.ensure((size_t)nb * p.cart_stride * sizeof(double)));
   CUDA_OK(p.d_vk.ensure((size_t)2 * nb * p.cart_stride * sizeof(double)));
+  CUDA_OK(p.d_dens_f.ensure((size_t)2 * nb * p.cart_stride * sizeof(float)));
   p.scratch_nb = nb;
 }
 
@@ -613,18 +741,6 @@ static void run_jk(Plan& p, const double* d_in, int nb, double* d_out, int with_
   ensure_scratch(p, nb);
   const int ndm = hermi ? nb : 2 * nb;
   const Tables tb = plan_tables(p);
-  // molecule AO starts (global cart / out AO index)
-  if (!p.d_mol_ao_off.ptr) {
-    std::vector<int> v(2 * p.nmol);
-    int c = 0, o = 0;
-    for (int m = 0; m < p.nmol; ++m) {
-      v[m] = c;
-      v[p.nmol + m] = o;
-      c += p.mol_ncart[m];
-      o += p.mol_nout[m];
-    }
-    upload(p.d_mol_ao_off, v.data(), v.size() * sizeof(int));
-  }
   const int* d_mol_cart_ao = p.d_mol_ao_off.as<int>();
   const int* d_mol_out_ao = d_mol_cart_ao + p.nmol;
   {
@@ -641,18 +757,22 @@ static void run_jk(Plan& p, const double* d_in, int nb, double* d_out, int with_
   if (with_j) CUDA_OK(cudaMemsetAsync(p.d_vj.ptr, 0, (size_t)nb * p.cart_stride * sizeof(double), st));
   if (with_k) CUDA_OK(cudaMemsetAsync(p.d_vk.ptr, 0, (size_t)ndm * p.cart_stride * sizeof(double), st));
   if (precision == B200JK_SPLIT) {
+    to_float_kernel<<<592, 256, 0, st>>>(p.d_dens.as<double>(), p.d_dens_f.as<float>(),
+                                         (long long)ndm * p.cart_stride);
+    CUDA_OK(cudaGetLastError());
     CUDA_OK(cudaMemsetAsync(p.d_maxd.ptr, 0, sizeof(double), st));
     maxabs_kernel<<<592, 256, 0, st>>>(d_in, (long long)nb * p.out_stride, p.d_maxd.as<double>());
     CUDA_OK(cudaGetLastError());
     for (auto* W : p.work) {
-      split_kernel<<<(W->nbra + 127) / 128, 128, 0, st>>>(
-          W->bra_kets.as<int2>(), p.classes[W->x].d_q.as<double>(), p.classes[W->y].d_q.as<double>(),
-          p.d_maxd.as<double>(), fp32_cut, W->nbra, W->split.as<int>());
+      split_kernel<<<(W->nwork + 127) / 128, 128, 0, st>>>(
+          W->work.as<int4>(), p.classes[W->x].d_q.as<double>(), p.classes[W->y].d_q.as<double>(),
+          p.d_maxd.as<double>(), fp32_cut, W->nwork, W->split.as<int>());
       CUDA_OK(cudaGetLastError());
     }
   }
   JKArgs a = base_args(p);
   a.dens = p.d_dens.as<double>();
+  a.dens_f = p.d_dens_f.as<float>();
   a.vj = p.d_vj.as<double>();
   a.vk = p.d_vk.as<double>();
   a.dstride = p.cart_stride;
@@ -668,17 +788,26 @@ static void run_jk(Plan& p, const double* d_in, int nb, double* d_out, int with_
     a.work = W->work.as<int4>();
     a.nwork = W->nwork;
     a.split = W->split.as<int>();
+    auto launch = [&](int mode, bool fp32) {
+      a.split_mode = mode;
+      ProfileEvent ev{cls, fp32 ? 1 : 0, nullptr, nullptr};
+      if (p.profiling) {
+        CUDA_OK(cudaEventCreate(&ev.start));
+        CUDA_OK(cudaEventCreate(&ev.stop));
+        CUDA_OK(cudaEventRecord(ev.start, st));
+      }
+      const int rc = fp32 ? disp.jk32[cls](a, st) : disp.jk64[cls](a, st);
+      if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+      if (p.profiling) {
+        CUDA_OK(cudaEventRecord(ev.stop, st));
+        p.events.push_back(ev);
+      }
+    };
     if (precision == B200JK_FP64) {
-      a.split_mode = 0;
-      const int rc = disp.jk64[cls](a, st);
-      if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+      launch(0, false);
     } else {
-      a.split_mode = 1;
-      int rc = disp.jk64[cls](a, st);
-      if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
-      a.split_mode = 2;
-      rc = disp.jk32[cls](a, st);
-      if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+      launch(1, false);
+      launch(2, true);
     }
   }
   {
@@ -802,6 +931,184 @@ int b200jk_direct_jk_tables(const int32_t* atm, int32_t natm, const int32_t* bas
     int st = 0;
     CUDA_OK(cudaMemcpy(&st, p->d_status.ptr, sizeof(int), cudaMemcpyDeviceToHost));
     if (st & 1) invalid("Nonfinite density");
+  });
+}
+
+int b200jk_plan_class_stats(const b200jk_plan* plan, int64_t* quartets, int64_t* prim_quartets) {
+  return guarded([&] {
+    if (!plan || !quartets || !prim_quartets) invalid("Invalid plan query");
+    std::fill(quartets, quartets + kQuartetClasses, 0);
+    std::fill(prim_quartets, prim_quartets + kQuartetClasses, 0);
+    for (auto* W : plan->p->work) {
+      const int c = quartet_class(W->x, W->y);
+      quartets[c] += W->quartets;
+      prim_quartets[c] += W->prim_quartets;
+    }
+  });
+}
+
+int b200jk_plan_split_stats(b200jk_plan* plan, void* stream, int64_t* q64, int64_t* q32,
+                            int64_t* pq64, int64_t* pq32) {
+  return guarded([&] {
+    if (!plan || !q64 || !q32 || !pq64 || !pq32) invalid("Invalid plan query");
+    Plan& p = *plan->p;
+    CUDA_OK(cudaSetDevice(p.device));
+    CUDA_OK(cudaStreamSynchronize((cudaStream_t)stream));
+    for (int c = 0; c < kQuartetClasses; ++c) q64[c] = q32[c] = pq64[c] = pq32[c] = 0;
+    for (auto* W : p.work) {
+      const int c = quartet_class(W->x, W->y);
+      std::vector<int> split(W->nwork);
+      CUDA_OK(cudaMemcpy(split.data(), W->split.ptr, W->nwork * sizeof(int), cudaMemcpyDeviceToHost));
+      const auto& pre = p.classes[W->y].npp_prefix;
+      for (int i = 0; i < W->nwork; ++i) {
+        const int4 it = W->h_items[i];
+        const int lo = it.y, hi = it.z;
+        const int sp = std::min(std::max(split[i], lo), hi);
+        const long long npa = p.pair_info[p.classes[W->x].pairs[it.x]].w;
+        q64[c] += sp - lo;
+        q32[c] += hi - sp;
+        pq64[c] += npa * (pre[sp] - pre[lo]);
+        pq32[c] += npa * (pre[hi] - pre[sp]);
+      }
+    }
+  });
+}
+
+int b200jk_int1e(b200jk_plan* plan, int32_t which, double* d_out, void* stream) {
+  return guarded([&] {
+    if (!plan || !d_out || which < 0 || which > 2) invalid("Invalid one-electron request");
+    Plan& p = *plan->p;
+    CUDA_OK(cudaSetDevice(p.device));
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_OK(p.d_one_scratch.ensure((size_t)3 * p.cart_stride * sizeof(double)));
+    double* raw = p.d_one_scratch.as<double>();
+    CUDA_OK(cudaMemsetAsync(raw, 0, (size_t)3 * p.cart_stride * sizeof(double), st));
+    OneArgs a = one_args(p);
+    a.out_s = raw;
+    a.out_t = raw + p.cart_stride;
+    a.out_v = raw + 2 * p.cart_stride;
+    for (int c = 0; c < kPairClasses; ++c) {
+      a.pairs = p.d_all_pairs[c].as<int>();
+      a.npairs = p.n_all_pairs[c];
+      launch_one_electron(c, false, a, st);
+      CUDA_OK(cudaGetLastError());
+    }
+    const Tables tb = plan_tables(p);
+    const int no = max_no(p);
+    dim3 grid((unsigned)(((long long)no * no + 255) / 256), p.nmol);
+    cart_to_out_kernel<<<grid, 256, 0, st>>>(raw + which * p.cart_stride, d_out,
+        p.d_mol_base_out.as<long long>(), p.d_mol_nout.as<int>(), p.d_mol_base_cart.as<long long>(),
+        p.d_mol_ncart.as<int>(), p.d_out_ws.as<int>(), p.d_ws_info.as<int4>(),
+        p.d_mol_ao_off.as<int>() + p.nmol, tb.c2s);
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int b200jk_int1e_grad(b200jk_plan* plan, const double* d_density, const double* d_energy_weighted,
+                      double* d_grad, void* stream) {
+  return guarded([&] {
+    if (!plan || !d_density || !d_energy_weighted || !d_grad) invalid("Invalid one-electron gradient request");
+    Plan& p = *plan->p;
+    CUDA_OK(cudaSetDevice(p.device));
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_OK(p.d_one_dens.ensure((size_t)2 * p.cart_stride * sizeof(double)));
+    double* raw = p.d_one_dens.as<double>();
+    const Tables tb = plan_tables(p);
+    const int nc = max_nc(p);
+    const double* ins[2] = {d_density, d_energy_weighted};
+    for (int k = 0; k < 2; ++k) {
+      dim3 grid((unsigned)(((long long)nc * nc + 255) / 256), p.nmol, 1);
+      density_in_kernel<<<grid, 256, 0, st>>>(
+          ins[k], 1, 1, raw + k * p.cart_stride, p.out_stride, p.cart_stride,
+          p.d_mol_base_out.as<long long>(), p.d_mol_nout.as<int>(), p.d_mol_base_cart.as<long long>(),
+          p.d_mol_ncart.as<int>(), p.d_cart_ws.as<int>(), p.d_ws_info.as<int4>(),
+          p.d_mol_ao_off.as<int>(), tb.c2s, p.d_status.as<int>());
+      CUDA_OK(cudaGetLastError());
+    }
+    CUDA_OK(cudaMemsetAsync(d_grad, 0, (size_t)p.total_atm * 3 * sizeof(double), st));
+    OneArgs a = one_args(p);
+    a.dm = raw;
+    a.wm = raw + p.cart_stride;
+    a.grad = d_grad;
+    for (int c = 0; c < kPairClasses; ++c) {
+      a.pairs = p.d_all_pairs[c].as<int>();
+      a.npairs = p.n_all_pairs[c];
+      launch_one_electron(c, true, a, st);
+      CUDA_OK(cudaGetLastError());
+    }
+  });
+}
+
+int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_t nb,
+                              const double* d_cot, int32_t with_j, int32_t with_k, double* d_grad,
+                              void* stream) {
+  return guarded([&] {
+    if (!plan || !d_density || !d_cot || !d_grad || nb < 1) invalid("Invalid direct J/K geometry product");
+    if ((with_j != 0 && with_j != 1) || (with_k != 0 && with_k != 1) || !(with_j || with_k))
+      invalid("Invalid direct J/K geometry product");
+    Plan& p = *plan->p;
+    CUDA_OK(cudaSetDevice(p.device));
+    cudaStream_t st = (cudaStream_t)stream;
+    ensure_scratch(p, nb);
+    const Tables tb = plan_tables(p);
+    // raw Cartesian D (d_dens), J cotangent (d_vj) and K cotangent (d_vk)
+    const int nc = max_nc(p);
+    dim3 grid((unsigned)(((long long)nc * nc + 255) / 256), p.nmol, nb);
+    auto to_raw = [&](const double* src, double* dst) {
+      mat_in_kernel<<<grid, 256, 0, st>>>(src, dst, p.out_stride, p.cart_stride,
+          p.d_mol_base_out.as<long long>(), p.d_mol_nout.as<int>(), p.d_mol_base_cart.as<long long>(),
+          p.d_mol_ncart.as<int>(), p.d_cart_ws.as<int>(), p.d_ws_info.as<int4>(), p.d_mol_ao_off.as<int>(),
+          tb.c2s);
+      CUDA_OK(cudaGetLastError());
+    };
+    to_raw(d_density, p.d_dens.as<double>());
+    if (with_j) to_raw(d_cot, p.d_vj.as<double>());
+    if (with_k) to_raw(d_cot + (size_t)(with_j ? nb : 0) * p.out_stride, p.d_vk.as<double>());
+    CUDA_OK(cudaMemsetAsync(d_grad, 0, (size_t)p.total_atm * 3 * sizeof(double), st));
+    JKArgs a = base_args(p);
+    a.dens = p.d_dens.as<double>();
+    a.dstride = p.cart_stride;
+    a.cot_j = with_j ? p.d_vj.as<double>() : nullptr;
+    a.cot_k = with_k ? p.d_vk.as<double>() : nullptr;
+    a.gnb = nb;
+    a.grad = d_grad;
+    const auto& disp = dispatch();
+    for (auto* W : p.work) {
+      const int cls = quartet_class(W->x, W->y);
+      a.bra_pairs = p.classes[W->x].d_pairs.as<int>();
+      a.ket_pairs = p.classes[W->y].d_pairs.as<int>();
+      a.work = W->work.as<int4>();
+      a.nwork = W->nwork;
+      a.split_mode = 0;
+      const int rc = disp.grad64[cls](a, st);
+      if (rc) throw Failure{B200JK_INTERNAL, std::string("gradient launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+    }
+  });
+}
+
+int b200jk_plan_set_profiling(b200jk_plan* plan, int32_t on) {
+  return guarded([&] {
+    if (!plan) invalid("Null plan");
+    plan->p->profiling = on != 0;
+  });
+}
+
+int b200jk_plan_profile(b200jk_plan* plan, double* ms64, double* ms32, int32_t* launches) {
+  return guarded([&] {
+    if (!plan || !ms64 || !ms32 || !launches) invalid("Invalid plan query");
+    Plan& p = *plan->p;
+    CUDA_OK(cudaSetDevice(p.device));
+    for (int c = 0; c < kQuartetClasses; ++c) { ms64[c] = ms32[c] = 0.0; launches[c] = 0; }
+    for (auto& e : p.events) {
+      CUDA_OK(cudaEventSynchronize(e.stop));
+      float ms = 0.f;
+      CUDA_OK(cudaEventElapsedTime(&ms, e.start, e.stop));
+      (e.fp32 ? ms32 : ms64)[e.cls] += ms;
+      launches[e.cls] += 1;
+      cudaEventDestroy(e.start);
+      cudaEventDestroy(e.stop);
+    }
+    p.events.clear();
   });
 }
 

@@ -2,6 +2,7 @@
 // compiled once per pair so the classes build in parallel) and registers
 // their launchers in the dispatch table.
 #include "dispatch.h"
+#include "grad_kernels.cuh"
 #include "jk_kernels.cuh"
 
 #if !defined(BRA_CLASS) || !defined(KET_CLASS)
@@ -74,6 +75,28 @@ int launch_schwarz(const JKArgs& args, int npairs, int cart, cudaStream_t stream
 }
 #endif
 
+template <int LA, int LB, int LC, int LD>
+int launch_grad(const JKArgs& args, cudaStream_t stream) {
+  if (args.nwork <= 0) return 0;
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  constexpr int TEAM = CI::NOUT <= 8 ? 4 : CI::NOUT <= 64 ? 8 : CI::NOUT <= 256 ? 16 : 32;
+  using GC = GradCfg<LA, LB, LC, LD, TEAM>;
+  constexpr size_t per_team = GC::bytes();
+  int teams = 128 / TEAM;
+  while (teams > 1 && per_team * teams > 200 * 1024) --teams;
+  const size_t smem = per_team * teams;
+  if (smem > 48 * 1024) {
+    static bool configured = false;
+    if (!configured) {
+      cudaFuncSetAttribute(grad_team_kernel<LA, LB, LC, LD, TEAM>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      configured = true;
+    }
+  }
+  grad_team_kernel<LA, LB, LC, LD, TEAM><<<args.nwork, teams * TEAM, smem, stream>>>(args);
+  return (int)cudaGetLastError();
+}
+
 constexpr int X = BRA_CLASS;
 constexpr int Y = KET_CLASS;
 static_assert(Y <= X, "ket class must not exceed bra class");
@@ -88,6 +111,7 @@ void REG_NAME(BRA_CLASS, KET_CLASS)(DispatchTable& t) {
   const int id = X * (X + 1) / 2 + Y;
   t.jk64[id] = &launch_class<XA, XB, YA, YB, double>;
   t.jk32[id] = &launch_class<XA, XB, YA, YB, float>;
+  t.grad64[id] = &launch_grad<XA, XB, YA, YB>;
   t.reg_path[id] = Policy<XA, XB, YA, YB>::REG;
   t.team[id] = Policy<XA, XB, YA, YB>::REG ? 1 : Policy<XA, XB, YA, YB>::TEAM;
 #if BRA_CLASS == KET_CLASS

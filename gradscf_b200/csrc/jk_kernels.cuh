@@ -25,16 +25,17 @@ struct JKArgs {
   const double4* sh_xyz;     // centre
   const int4* pair_info;     // (shell A, shell B, first primitive pair, count)
   const double4* pp_data;    // primitive pair: (Px, Py, Pz, p = a+b)
-  const double* pp_k;        // exp(-ab/p |AB|^2) * c_a * c_b
+  const double2* pp_aux;     // (exp(-ab/p |AB|^2) c_a c_b / p, 1/(2p))
   const long long* mol_base; // offset of the molecule's n x n block
   const int* mol_n;          // Cartesian AO count of the molecule
   const int* bra_pairs;      // sorted pair ids of the bra class
   const int* ket_pairs;      // sorted pair ids of the ket class
   const int4* work;          // (bra position, ket begin, ket end, unused)
   int nwork;
-  const int* split;          // per bra position: first ket computed in FP32
+  const int* split;          // per work item: first ket computed in FP32
   int split_mode;            // 0 all kets, 1 kets below split, 2 kets from split
   const double* dens;        // [ndm][dstride] Cartesian effective densities
+  const float* dens_f;       // the same in FP32 (used by FP32 quartets)
   double* vj;                // [nsym][dstride]
   double* vk;                // [ndm][dstride]
   long long dstride;
@@ -42,6 +43,21 @@ struct JKArgs {
   Tables tb;
   double* q_out;             // Schwarz mode: per pair max |(ab|ab)| in output basis
   int* status;               // device error word (0 = ok)
+  // coordinate VJP
+  const double2* pp_exp;     // primitive pair: (exponent on A, exponent on B)
+  const double* cot_j;       // raw Cartesian J cotangents [gnb][dstride] (or null)
+  const double* cot_k;       // raw Cartesian K cotangents (or null)
+  int gnb;                   // density / cotangent batches
+  const int* ws_atm;         // atm row of each work shell's centre
+  double* grad;              // (atm rows, 3)
+};
+
+template <typename R> struct DensSel;
+template <> struct DensSel<double> {
+  static __device__ __forceinline__ const double* get(const JKArgs& a) { return a.dens; }
+};
+template <> struct DensSel<float> {
+  static __device__ __forceinline__ const float* get(const JKArgs& a) { return a.dens_f; }
 };
 
 template <int LA, int LB, int LC, int LD>
@@ -56,7 +72,7 @@ __device__ __forceinline__ void ket_range(const JKArgs& args, const int4 w, int&
   kb = w.y;
   ke = w.z;
   if (args.split_mode != 0) {
-    const int s = args.split[w.x];
+    const int s = args.split[blockIdx.x];
     if (args.split_mode == 1) ke = min(ke, s);
     else kb = max(kb, s);
   }
@@ -102,24 +118,43 @@ struct PrimQ {
   R t, pref;
 };
 
+// Division-free: pref = 2 pi^2.5 (K_ab/p)(K_cd/q) / sqrt(p+q) with the
+// per-pair factors precomputed; 1/(p+q) = rsqrt(p+q)^2.
 template <typename R>
-__device__ __forceinline__ void prim_setup(const JKArgs& args, const QuartetGeom& g, int i, int j,
-                                           PrimQ<R>& s) {
-  const double4 P = args.pp_data[i];
-  const double4 Q = args.pp_data[j];
-  const double kab = args.pp_k[i], kcd = args.pp_k[j];
+__device__ __forceinline__ void prim_setup(const QuartetGeom& g, const double4 P, const double2 PA,
+                                           const double4 Q, const double2 QA, PrimQ<R>& s) {
+  if constexpr (sizeof(R) == 4) {
+    // FP32 quartets: centre differences in FP64, the rest in FP32.
+    const float p = float(P.w), q = float(Q.w);
+    const float pq = p + q;
+    const float rs = rsqrtf(pq);
+    const float ipq = rs * rs;
+    const float pqx = float(P.x - Q.x), pqy = float(P.y - Q.y), pqz = float(P.z - Q.z);
+    s.t = p * q * ipq * (pqx * pqx + pqy * pqy + pqz * pqz);
+    s.pref = float(B200JK_ERI_C0) * float(PA.x) * float(QA.x) * rs;
+    s.pq_inv = ipq;
+    s.q_pq = q * ipq;
+    s.p_pq = p * ipq;
+    s.inv2p = float(PA.y);
+    s.inv2q = float(QA.y);
+    s.pax = float(P.x - g.ax); s.pay = float(P.y - g.ay); s.paz = float(P.z - g.az);
+    s.qcx = float(Q.x - g.cx); s.qcy = float(Q.y - g.cy); s.qcz = float(Q.z - g.cz);
+    s.pqx = pqx; s.pqy = pqy; s.pqz = pqz;
+    return;
+  }
   const double p = P.w, q = Q.w;
   const double pq = p + q;
+  const double rs = rsqrt(pq);
+  const double ipq = rs * rs;
   const double pqx = P.x - Q.x, pqy = P.y - Q.y, pqz = P.z - Q.z;
-  const double rho = p * q / pq;
-  const double t = rho * (pqx * pqx + pqy * pqy + pqz * pqz);
+  const double t = p * q * ipq * (pqx * pqx + pqy * pqy + pqz * pqz);
   s.t = R(t);
-  s.pref = R(B200JK_ERI_C0 * kab * kcd / (p * q * sqrt(pq)));
-  s.pq_inv = R(1.0 / pq);
-  s.q_pq = R(q / pq);
-  s.p_pq = R(p / pq);
-  s.inv2p = R(0.5 / p);
-  s.inv2q = R(0.5 / q);
+  s.pref = R(B200JK_ERI_C0 * PA.x * QA.x * rs);
+  s.pq_inv = R(ipq);
+  s.q_pq = R(q * ipq);
+  s.p_pq = R(p * ipq);
+  s.inv2p = R(PA.y);
+  s.inv2q = R(QA.y);
   s.pax = R(P.x - g.ax); s.pay = R(P.y - g.ay); s.paz = R(P.z - g.az);
   s.qcx = R(Q.x - g.cx); s.qcy = R(Q.y - g.cy); s.qcz = R(Q.z - g.cz);
   s.pqx = R(pqx); s.pqy = R(pqy); s.pqz = R(pqz);
@@ -156,16 +191,18 @@ __device__ __forceinline__ long long dm_index(const JKArgs& args, int mol, int a
 // ---------------------------------------------------------------------------
 template <int LA, int LB, int LC, int LD, typename R>
 __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const QuartetGeom& g,
-                                                  R* out) {
+                                                  const double4* bpp, const double2* baux, R* out) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   using GI = GIdx<LA, LB, LC, LD>;
   constexpr int N = CI::NROOT;
 #pragma unroll
   for (int o = 0; o < CI::NOUT; ++o) out[o] = R(0);
-  for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
+  for (int i = 0; i < g.npa; ++i) {
+    const double4 P = bpp[i];
+    const double2 PA = baux[i];
     for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
       PrimQ<R> s;
-      prim_setup<R>(args, g, i, j, s);
+      prim_setup<R>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
       R x[N], w[N];
       rys_roots<N, R>(s.t, x, w, args.tb);
 #pragma unroll
@@ -198,139 +235,175 @@ __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const Quar
   }
 }
 
+// J[a][b] of the block's bra pair for density 0 goes to `jab` (reduced by
+// the caller) when acc_j is set; everything else is an atomic add.  Density
+// elements are read where they are used (L1/L2 resident).
 template <int LA, int LB, int LC, int LD, typename R>
-__device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom& g, const R* out) {
+__device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom& g, const R* out,
+                                           bool acc_j, double* jab) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   constexpr int NA = CI::NA, NB = CI::NB, NC = CI::NC, ND = CI::ND;
   const double s = g.scale;
   const long long base = args.mol_base[g.mol];
   const int n = args.mol_n[g.mol];
+  // per-quartet contractions in R (FP32 quartets: FP32 accumulation per
+  // quartet); the J/K matrices themselves are accumulated in FP64.
+  const R* dens = DensSel<R>::get(args);
+#define V_(a, b, c, d) (out[(((a) * NB + (b)) * NC + (c)) * ND + (d)])
   for (int e = 0; e < args.ndm; ++e) {
-    const double* dm = args.dens + e * args.dstride + base;
+    const R* dm = dens + e * args.dstride + base;
     if (args.with_j && e < args.nsym) {
       double* vj = args.vj + e * args.dstride + base;
-      double dab[NA * NB], dcd[NC * ND];
 #pragma unroll
       for (int a = 0; a < NA; ++a)
 #pragma unroll
-        for (int b = 0; b < NB; ++b) dab[a * NB + b] = dm[(long long)(g.aoA + a) * n + g.aoB + b];
+        for (int b = 0; b < NB; ++b) {
+          R acc = R(0);
+#pragma unroll
+          for (int c = 0; c < NC; ++c)
+#pragma unroll
+            for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoC + c) * n + g.aoD + d);
+          if (acc_j && e == 0) jab[a * NB + b] = 2.0 * s * double(acc);
+          else atomicAdd(vj + (long long)(g.aoA + a) * n + g.aoB + b, 2.0 * s * double(acc));
+        }
 #pragma unroll
       for (int c = 0; c < NC; ++c)
 #pragma unroll
-        for (int d = 0; d < ND; ++d) dcd[c * ND + d] = dm[(long long)(g.aoC + c) * n + g.aoD + d];
+        for (int d = 0; d < ND; ++d) {
+          R acc = R(0);
 #pragma unroll
-      for (int ab = 0; ab < NA * NB; ++ab) {
-        double acc = 0.0;
+          for (int a = 0; a < NA; ++a)
 #pragma unroll
-        for (int cd = 0; cd < NC * ND; ++cd) acc += double(out[ab * NC * ND + cd]) * dcd[cd];
-        atomicAdd(vj + (long long)(g.aoA + ab / NB) * n + g.aoB + ab % NB, 2.0 * s * acc);
-      }
-#pragma unroll
-      for (int cd = 0; cd < NC * ND; ++cd) {
-        double acc = 0.0;
-#pragma unroll
-        for (int ab = 0; ab < NA * NB; ++ab) acc += double(out[ab * NC * ND + cd]) * dab[ab];
-        atomicAdd(vj + (long long)(g.aoC + cd / ND) * n + g.aoD + cd % ND, 2.0 * s * acc);
-      }
+            for (int b = 0; b < NB; ++b) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoA + a) * n + g.aoB + b);
+          atomicAdd(vj + (long long)(g.aoC + c) * n + g.aoD + d, 2.0 * s * double(acc));
+        }
     }
     if (args.with_k) {
       double* vk = args.vk + e * args.dstride + base;
-      // K[a][c] += s sum_bd V D[b][d]
-      {
-        double dbd[NB * ND];
 #pragma unroll
-        for (int b = 0; b < NB; ++b)
+      for (int a = 0; a < NA; ++a)
 #pragma unroll
-          for (int d = 0; d < ND; ++d) dbd[b * ND + d] = dm[(long long)(g.aoB + b) * n + g.aoD + d];
+        for (int c = 0; c < NC; ++c) {
+          R acc = R(0);
 #pragma unroll
-        for (int a = 0; a < NA; ++a)
+          for (int b = 0; b < NB; ++b)
 #pragma unroll
-          for (int c = 0; c < NC; ++c) {
-            double acc = 0.0;
+            for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoB + b) * n + g.aoD + d);
+          atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoC + c, s * double(acc));
+        }
 #pragma unroll
-            for (int b = 0; b < NB; ++b)
+      for (int a = 0; a < NA; ++a)
 #pragma unroll
-              for (int d = 0; d < ND; ++d)
-                acc += double(out[((a * NB + b) * NC + c) * ND + d]) * dbd[b * ND + d];
-            atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoC + c, s * acc);
-          }
-      }
-      // K[a][d] += s sum_bc V D[b][c]
-      {
-        double dbc[NB * NC];
+        for (int d = 0; d < ND; ++d) {
+          R acc = R(0);
 #pragma unroll
-        for (int b = 0; b < NB; ++b)
+          for (int b = 0; b < NB; ++b)
 #pragma unroll
-          for (int c = 0; c < NC; ++c) dbc[b * NC + c] = dm[(long long)(g.aoB + b) * n + g.aoC + c];
+            for (int c = 0; c < NC; ++c) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoB + b) * n + g.aoC + c);
+          atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoD + d, s * double(acc));
+        }
 #pragma unroll
-        for (int a = 0; a < NA; ++a)
+      for (int b = 0; b < NB; ++b)
 #pragma unroll
-          for (int d = 0; d < ND; ++d) {
-            double acc = 0.0;
+        for (int c = 0; c < NC; ++c) {
+          R acc = R(0);
 #pragma unroll
-            for (int b = 0; b < NB; ++b)
+          for (int a = 0; a < NA; ++a)
 #pragma unroll
-              for (int c = 0; c < NC; ++c)
-                acc += double(out[((a * NB + b) * NC + c) * ND + d]) * dbc[b * NC + c];
-            atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoD + d, s * acc);
-          }
-      }
-      // K[b][c] += s sum_ad V D[a][d]
-      {
-        double dad[NA * ND];
+            for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoA + a) * n + g.aoD + d);
+          atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoC + c, s * double(acc));
+        }
 #pragma unroll
-        for (int a = 0; a < NA; ++a)
+      for (int b = 0; b < NB; ++b)
 #pragma unroll
-          for (int d = 0; d < ND; ++d) dad[a * ND + d] = dm[(long long)(g.aoA + a) * n + g.aoD + d];
+        for (int d = 0; d < ND; ++d) {
+          R acc = R(0);
 #pragma unroll
-        for (int b = 0; b < NB; ++b)
+          for (int a = 0; a < NA; ++a)
 #pragma unroll
-          for (int c = 0; c < NC; ++c) {
-            double acc = 0.0;
-#pragma unroll
-            for (int a = 0; a < NA; ++a)
-#pragma unroll
-              for (int d = 0; d < ND; ++d)
-                acc += double(out[((a * NB + b) * NC + c) * ND + d]) * dad[a * ND + d];
-            atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoC + c, s * acc);
-          }
-      }
-      // K[b][d] += s sum_ac V D[a][c]
-      {
-        double dac[NA * NC];
-#pragma unroll
-        for (int a = 0; a < NA; ++a)
-#pragma unroll
-          for (int c = 0; c < NC; ++c) dac[a * NC + c] = dm[(long long)(g.aoA + a) * n + g.aoC + c];
-#pragma unroll
-        for (int b = 0; b < NB; ++b)
-#pragma unroll
-          for (int d = 0; d < ND; ++d) {
-            double acc = 0.0;
-#pragma unroll
-            for (int a = 0; a < NA; ++a)
-#pragma unroll
-              for (int c = 0; c < NC; ++c)
-                acc += double(out[((a * NB + b) * NC + c) * ND + d]) * dac[a * NC + c];
-            atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoD + d, s * acc);
-          }
-      }
+            for (int c = 0; c < NC; ++c) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoA + a) * n + g.aoC + c);
+          atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoD + d, s * double(acc));
+        }
     }
   }
+#undef V_
 }
 
+// Occupancy target of the register path from its estimated register need.
 template <int LA, int LB, int LC, int LD, typename R>
-__global__ void __launch_bounds__(128) jk_reg_kernel(JKArgs args) {
+struct RegMinBlocks {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  static constexpr int EST = 2 * (CI::NOUT + 3 * CI::NG) + 56;   // same cap for FP32 and FP64
+  static constexpr int value = EST <= 120 ? 4 : (EST <= 150 ? 3 : 2);
+};
+
+constexpr int kBraPrimCache = 128;
+
+template <int LA, int LB, int LC, int LD, typename R>
+__global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
+    jk_reg_kernel(JKArgs args) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  __shared__ double4 s_pp[kBraPrimCache];
+  __shared__ double2 s_aux[kBraPrimCache];
   const int4 w = args.work[blockIdx.x];
   int kb, ke;
   ket_range(args, w, kb, ke);
+  if (kb >= ke) return;
   const int bra = args.bra_pairs[w.x];
-  for (int k = kb + threadIdx.x; k < ke; k += blockDim.x) {
-    QuartetGeom g;
-    load_quartet(args, bra, args.ket_pairs[k], g);
-    R out[ClassInfo<LA, LB, LC, LD>::NOUT];
-    quartet_block_reg<LA, LB, LC, LD, R>(args, g, out);
-    digest_reg<LA, LB, LC, LD, R>(args, g, out);
+  const int4 pb = args.pair_info[bra];
+  const bool cached = pb.w <= kBraPrimCache;
+  if (cached) {
+    for (int i = threadIdx.x; i < pb.w; i += blockDim.x) {
+      s_pp[i] = args.pp_data[pb.z + i];
+      s_aux[i] = args.pp_aux[pb.z + i];
+    }
+  }
+  __syncthreads();
+  const double4* bpp = cached ? s_pp : args.pp_data + pb.z;
+  const double2* baux = cached ? s_aux : args.pp_aux + pb.z;
+  // J[a][b] of the fixed bra pair (single symmetric density): each loop
+  // iteration reduces the 32 lanes' contributions with shuffles into the
+  // warp's shared row; the rows are summed and added once per block.
+  __shared__ double s_jab[4][CI::NAB];
+  const bool acc_j = args.with_j && args.nsym == 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (acc_j && lane < CI::NAB) s_jab[warp][lane] = 0.0;
+  if (acc_j && CI::NAB > 32)
+    for (int i = lane + 32; i < CI::NAB; i += 32) s_jab[warp][i] = 0.0;
+  QuartetGeom g;
+  for (int k0 = kb; k0 < ke; k0 += blockDim.x) {
+    const int k = k0 + threadIdx.x;
+    double jab[CI::NAB];
+#pragma unroll
+    for (int i = 0; i < CI::NAB; ++i) jab[i] = 0.0;
+    if (k < ke) {
+      load_quartet(args, bra, args.ket_pairs[k], g);
+      R out[CI::NOUT];
+      quartet_block_reg<LA, LB, LC, LD, R>(args, g, bpp, baux, out);
+      digest_reg<LA, LB, LC, LD, R>(args, g, out, acc_j, jab);
+    }
+    if (acc_j) {
+#pragma unroll
+      for (int ab = 0; ab < CI::NAB; ++ab) {
+        double v = jab[ab];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) s_jab[warp][ab] += v;
+      }
+    }
+  }
+  if (acc_j) {
+    __syncthreads();
+    const int4 ia = args.sh_info[pb.x], ib = args.sh_info[pb.y];
+    const long long base = args.mol_base[ia.z];
+    const int n = args.mol_n[ia.z];
+    double* vj = args.vj + base;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int ab = threadIdx.x; ab < CI::NAB; ab += blockDim.x) {
+      double v = 0.0;
+      for (int i = 0; i < nw; ++i) v += s_jab[i][ab];
+      if (v != 0.0) atomicAdd(vj + (long long)(ia.x + ab / CI::NB) * n + ib.x + ab % CI::NB, v);
+    }
   }
 }
 
@@ -384,9 +457,11 @@ __device__ __forceinline__ void team_block(const JKArgs& args, const QuartetGeom
       }
     }
     for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
+      const double4 P = args.pp_data[i];
+      const double2 PA = args.pp_aux[i];
       for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
         PrimQ<R> s;
-        prim_setup<R>(args, g, i, j, s);
+        prim_setup<R>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
         for (int f = lane; f < 2 * N; f += TEAM) roots[f] = rys_one<N, R>(s.t, f, args.tb);
         __syncwarp(mask);
         for (int tsk = lane; tsk < 3 * N; tsk += TEAM) {

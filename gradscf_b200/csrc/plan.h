@@ -37,16 +37,25 @@ struct ClassPairWork {
   int nwork = 0;
   int nbra = 0;
   DevBuf work;                  // int4 per work item
-  DevBuf bra_kets;              // int2 per bra position: [ket lo, ket hi)
-  DevBuf split;                 // int per bra position (filled per call)
-  long long quartets = 0;       // significant quartets in this class pair
+  DevBuf split;                 // int per work item: first FP32 ket (filled per call)
+  long long quartets = 0;       // significant work-shell quartets in this class pair
+  long long prim_quartets = 0;  // their primitive quartets
+  std::vector<int4> h_items;    // host copy of the work items
 };
 
 struct ClassList {
   std::vector<int> pairs;       // pair ids, sorted (molecule, Q desc)
   std::vector<double> q;        // their parent Schwarz bounds
   std::vector<int> mol_begin;   // per molecule: first position (size nmol+1)
+  std::vector<std::vector<int2>> segs;  // per molecule: [begin, end) runs of equal primitive-pair count
+  std::vector<long long> npp_prefix;  // prefix sums of primitive-pair counts (size+1)
   DevBuf d_pairs, d_q;
+};
+
+struct ProfileEvent {
+  int cls;
+  int fp32;
+  cudaEvent_t start, stop;
 };
 
 struct Plan {
@@ -79,14 +88,27 @@ struct Plan {
   // nuclei (for one-electron terms): global atm rows with charge
   std::vector<double4> atom_xyzq; // (x, y, z, charge) per global atm row
   // device tables
-  DevBuf d_ws_info, d_ws_xyz, d_pair_info, d_pp_data, d_pp_k, d_mol_base_cart, d_mol_ncart,
+  DevBuf d_ws_info, d_ws_xyz, d_pair_info, d_pp_data, d_pp_aux, d_pp_exp, d_mol_base_cart, d_mol_ncart,
       d_mol_base_out, d_mol_nout, d_cart_ws, d_out_ws, d_status, d_maxd, d_q_work, d_atoms,
       d_ws_atm, d_mol_ao_off, d_ws_prim, d_ws_prim_off;
+  // one-electron work: every work pair of each pair class, nuclei ranges
+  DevBuf d_all_pairs[kPairClasses];
+  int n_all_pairs[kPairClasses] = {};
+  DevBuf d_mol_atm, d_mol_natm;
+  DevBuf d_one_scratch;           // raw Cartesian S, T, V (3 x cart_stride)
+  DevBuf d_one_dens;              // raw Cartesian D, W (2 x cart_stride)
   // scratch
-  DevBuf d_dens, d_vj, d_vk;
+  DevBuf d_dens, d_dens_f, d_vj, d_vk;
   int scratch_nb = 0;
+  // optional per-class launch timing (CUDA events on the launching stream)
+  bool profiling = false;
+  std::vector<ProfileEvent> events;
   ~Plan() {
     for (auto* w : work) delete w;
+    for (auto& e : events) {
+      cudaEventDestroy(e.start);
+      cudaEventDestroy(e.stop);
+    }
   }
 };
 

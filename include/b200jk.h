@@ -69,6 +69,27 @@ int b200jk_plan_quartets(const b200jk_plan* plan, int64_t* count);
  * (molecule m occupies [offset[m], offset[m] + nao[m]^2) of each matrix). */
 int b200jk_plan_block_offsets(const b200jk_plan* plan, int64_t* offsets);
 
+/* Per angular-momentum class pair (index x(x+1)/2 + y of the pair classes
+ * x >= y, pair class l_a(l_a+1)/2 + l_b; 55 entries): significant quartets of
+ * split-contraction shells and their primitive quartets.  For the FLOP model. */
+int b200jk_plan_class_stats(const b200jk_plan* plan, int64_t* quartets, int64_t* prim_quartets);
+
+/* After a B200JK_SPLIT call (synchronises `stream`): per class pair, the
+ * quartets and primitive quartets that ran in FP64 and in FP32. */
+int b200jk_plan_split_stats(b200jk_plan* plan, void* stream, int64_t* q64, int64_t* q32,
+                            int64_t* pq64, int64_t* pq32);
+
+/* Optional CUDA-event timing of every class-pair launch (on the launching
+ * stream).  b200jk_plan_profile synchronises, returns per class pair the
+ * summed milliseconds of FP64 and FP32 launches and the launch counts since
+ * the last read, then resets. */
+int b200jk_plan_set_profiling(b200jk_plan* plan, int32_t on);
+int b200jk_plan_profile(b200jk_plan* plan, double* ms64, double* ms32, int32_t* launches);
+
+/* Measured vector-pipe FMA throughput of the current device in TFLOP/s
+ * (fp64 = 1: FP64, 0: FP32) -- the roofline denominator for the ERI kernels. */
+int b200jk_measure_fma_peak(int32_t fp64, double* tflops, void* stream);
+
 /* Direct J/K (replaces GradSCFDirectJK, csrc/direct_jk.cc:7-95).
  *   d_density : device, nb packed density sets (nb x sum_m nao_m^2, row-major
  *               per molecule; for one molecule simply (nb, n, n)).  Need not be
