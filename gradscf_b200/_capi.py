@@ -20,7 +20,9 @@ EXPORTS = (
     "b200jk_check_status", "b200jk_direct_jk_tables", "b200jk_direct_jk_geom_vjp",
     "b200jk_int1e", "b200jk_int1e_grad", "b200jk_plan_class_stats", "b200jk_plan_split_stats",
     "b200jk_plan_set_profiling", "b200jk_plan_profile", "b200jk_measure_fma_peak",
+    "b200jk_direct_jk_noalloc",
 )
+NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024
 NCLASS = 55
 PAIR_CLASSES = ((0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2), (3, 0), (3, 1), (3, 2), (3, 3))
 QUARTET_CLASSES = tuple(PAIR_CLASSES[x] + PAIR_CLASSES[y] for x in range(10) for y in range(x + 1))
@@ -76,6 +78,7 @@ def lib():
     h.b200jk_plan_set_profiling.argtypes = [vp, i32]
     h.b200jk_plan_profile.argtypes = [vp, ctypes.POINTER(f64), ctypes.POINTER(f64), ctypes.POINTER(i32)]
     h.b200jk_measure_fma_peak.argtypes = [i32, ctypes.POINTER(f64), vp]
+    h.b200jk_direct_jk_noalloc.argtypes = [vp, vp, i32, vp, i32, i32, i32, i32, f64, vp]
     return h
 
 

@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -729,16 +730,23 @@ static void ensure_scratch(Plan& p, int nb) {
 static int max_nc(const Plan& p) { return *std::max_element(p.mol_ncart.begin(), p.mol_ncart.end()); }
 static int max_no(const Plan& p) { return *std::max_element(p.mol_nout.begin(), p.mol_nout.end()); }
 
-static void run_jk(Plan& p, const double* d_in, int nb, double* d_out, int with_j, int with_k,
-                   int hermi, int precision, double fp32_cut, cudaStream_t st) {
+void check_jk_args(const Plan& p, const double* d_in, int nb, const double* d_out, int with_j,
+                   int with_k, int precision, double fp32_cut) {
+  (void)p;
   if (nb < 1) invalid("Direct J/K requires at least one density");
   if ((with_j != 0 && with_j != 1) || (with_k != 0 && with_k != 1) || !(with_j || with_k))
     invalid("Direct J/K requires at least one selected operator");
   if (precision != B200JK_FP64 && precision != B200JK_SPLIT) invalid("Unknown precision mode");
   if (precision == B200JK_SPLIT && !(fp32_cut >= 0 && std::isfinite(fp32_cut))) invalid("Invalid fp32_cut");
   if (!d_in || !d_out) invalid("Null density or output pointer");
-  CUDA_OK(cudaSetDevice(p.device));
-  ensure_scratch(p, nb);
+}
+
+// The J/K pipeline on caller-provided scratch: dens/dens_f hold (hermi ? nb :
+// 2nb) Cartesian matrices, vj nb, vk (hermi ? nb : 2nb); nothing is allocated
+// here when profiling is off.
+void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j, int with_k,
+                 int hermi, int precision, double fp32_cut, cudaStream_t st, double* s_dens,
+                 float* s_dens_f, double* s_vj, double* s_vk, bool allow_profiling) {
   const int ndm = hermi ? nb : 2 * nb;
   const Tables tb = plan_tables(p);
   const int* d_mol_cart_ao = p.d_mol_ao_off.as<int>();
@@ -748,16 +756,16 @@ static void run_jk(Plan& p, const double* d_in, int nb, double* d_out, int with_
     const long long n2 = (long long)nc * nc;
     dim3 grid((unsigned)((n2 + 255) / 256), p.nmol, nb);
     density_in_kernel<<<grid, 256, 0, st>>>(
-        d_in, nb, hermi, p.d_dens.as<double>(), p.out_stride, p.cart_stride,
+        d_in, nb, hermi, s_dens, p.out_stride, p.cart_stride,
         p.d_mol_base_out.as<long long>(), p.d_mol_nout.as<int>(), p.d_mol_base_cart.as<long long>(),
         p.d_mol_ncart.as<int>(), p.d_cart_ws.as<int>(), p.d_ws_info.as<int4>(), d_mol_cart_ao, tb.c2s,
         p.d_status.as<int>());
     CUDA_OK(cudaGetLastError());
   }
-  if (with_j) CUDA_OK(cudaMemsetAsync(p.d_vj.ptr, 0, (size_t)nb * p.cart_stride * sizeof(double), st));
-  if (with_k) CUDA_OK(cudaMemsetAsync(p.d_vk.ptr, 0, (size_t)ndm * p.cart_stride * sizeof(double), st));
+  if (with_j) CUDA_OK(cudaMemsetAsync(s_vj, 0, (size_t)nb * p.cart_stride * sizeof(double), st));
+  if (with_k) CUDA_OK(cudaMemsetAsync(s_vk, 0, (size_t)ndm * p.cart_stride * sizeof(double), st));
   if (precision == B200JK_SPLIT) {
-    to_float_kernel<<<592, 256, 0, st>>>(p.d_dens.as<double>(), p.d_dens_f.as<float>(),
+    to_float_kernel<<<592, 256, 0, st>>>(s_dens, s_dens_f,
                                          (long long)ndm * p.cart_stride);
     CUDA_OK(cudaGetLastError());
     CUDA_OK(cudaMemsetAsync(p.d_maxd.ptr, 0, sizeof(double), st));
@@ -771,10 +779,10 @@ static void run_jk(Plan& p, const double* d_in, int nb, double* d_out, int with_
     }
   }
   JKArgs a = base_args(p);
-  a.dens = p.d_dens.as<double>();
-  a.dens_f = p.d_dens_f.as<float>();
-  a.vj = p.d_vj.as<double>();
-  a.vk = p.d_vk.as<double>();
+  a.dens = s_dens;
+  a.dens_f = s_dens_f;
+  a.vj = s_vj;
+  a.vk = s_vk;
   a.dstride = p.cart_stride;
   a.ndm = ndm;
   a.nsym = nb;
@@ -791,14 +799,14 @@ static void run_jk(Plan& p, const double* d_in, int nb, double* d_out, int with_
     auto launch = [&](int mode, bool fp32) {
       a.split_mode = mode;
       ProfileEvent ev{cls, fp32 ? 1 : 0, nullptr, nullptr};
-      if (p.profiling) {
+      if (p.profiling && allow_profiling) {
         CUDA_OK(cudaEventCreate(&ev.start));
         CUDA_OK(cudaEventCreate(&ev.stop));
         CUDA_OK(cudaEventRecord(ev.start, st));
       }
       const int rc = fp32 ? disp.jk32[cls](a, st) : disp.jk64[cls](a, st);
       if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
-      if (p.profiling) {
+      if (p.profiling && allow_profiling) {
         CUDA_OK(cudaEventRecord(ev.stop, st));
         p.events.push_back(ev);
       }
@@ -815,12 +823,21 @@ static void run_jk(Plan& p, const double* d_in, int nb, double* d_out, int with_
     const long long n2 = (long long)no * no;
     dim3 grid((unsigned)((n2 + 255) / 256), p.nmol, nb);
     jk_out_kernel<<<grid, 256, 0, st>>>(
-        p.d_vj.as<double>(), p.d_vk.as<double>(), nb, hermi, with_j, with_k, d_out, p.out_stride,
+        s_vj, s_vk, nb, hermi, with_j, with_k, d_out, p.out_stride,
         p.cart_stride, p.d_mol_base_out.as<long long>(), p.d_mol_nout.as<int>(),
         p.d_mol_base_cart.as<long long>(), p.d_mol_ncart.as<int>(), p.d_out_ws.as<int>(),
         p.d_ws_info.as<int4>(), d_mol_out_ao, tb.c2s);
     CUDA_OK(cudaGetLastError());
   }
+}
+
+static void run_jk(Plan& p, const double* d_in, int nb, double* d_out, int with_j, int with_k,
+                   int hermi, int precision, double fp32_cut, cudaStream_t st) {
+  check_jk_args(p, d_in, nb, d_out, with_j, with_k, precision, fp32_cut);
+  CUDA_OK(cudaSetDevice(p.device));
+  ensure_scratch(p, nb);
+  run_jk_core(p, d_in, nb, d_out, with_j, with_k, hermi, precision, fp32_cut, st, p.d_dens.as<double>(),
+              p.d_dens_f.as<float>(), p.d_vj.as<double>(), p.d_vk.as<double>(), true);
 }
 
 template <typename F>
@@ -841,13 +858,12 @@ static int guarded(F&& f) {
   }
 }
 
+int guarded_call(const std::function<void()>& f) { return guarded(f); }
+void fail_invalid(const std::string& m) { invalid(m); }
+
 }  // namespace b200jk
 
 using namespace b200jk;
-
-struct b200jk_plan {
-  Plan* p;
-};
 
 extern "C" {
 

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -112,9 +113,22 @@ struct Plan {
   }
 };
 
+void check_jk_args(const Plan& p, const double* d_in, int nb, const double* d_out, int with_j,
+                   int with_k, int precision, double fp32_cut);
+void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j, int with_k,
+                 int hermi, int precision, double fp32_cut, cudaStream_t st, double* s_dens,
+                 float* s_dens_f, double* s_vj, double* s_vk, bool allow_profiling);
+int guarded_call(const std::function<void()>& f);
+void fail_invalid(const std::string& m);
+
 // Device-wide constant tables (Rys, Boys, c2s) of the current device.
 const Tables& device_tables(int device);
 
 void set_error(const std::string& msg);
 
 }  // namespace b200jk
+
+// The C ABI's opaque plan handle.
+struct b200jk_plan {
+  b200jk::Plan* p;
+};

@@ -104,6 +104,23 @@ int b200jk_direct_jk(b200jk_plan* plan, const double* d_density, int32_t nb, dou
                      int32_t with_j, int32_t with_k, int32_t hermi, int32_t precision,
                      double fp32_cut, void* stream);
 
+/* Allocation-free variant of b200jk_direct_jk.  No counterpart in the
+ * reference (its CPU handler allocates per call).  For callers that may not
+ * allocate device memory while they run -- an XLA custom call on a stream
+ * XLA owns, code inside CUDA stream capture, a host with a fixed memory
+ * budget.  Same arguments and results as b200jk_direct_jk, but the scratch
+ * (effective densities and J/K accumulators) lives in a static device array
+ * of B200JK_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
+ * until exit; a call needing more returns B200JK_INVALID_ARGUMENT with the
+ * byte counts.  The plan must already exist (plan creation allocates).
+ * All calls share the array: calls that overlap on the GPU race, so order
+ * them on one stream.  The first call on a device looks up the array's
+ * address with that device current -- make it before any stream capture. */
+#define B200JK_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int b200jk_direct_jk_noalloc(b200jk_plan* plan, const double* d_density, int32_t nb, double* d_out,
+                             int32_t with_j, int32_t with_k, int32_t hermi, int32_t precision,
+                             double fp32_cut, void* stream);
+
 /* Synchronise `stream` and turn the plan's device status word into a return
  * code (nonfinite density -> B200JK_INVALID_ARGUMENT), clearing it. */
 int b200jk_check_status(b200jk_plan* plan, void* stream);
