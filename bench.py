@@ -1,25 +1,31 @@
-"""Benchmark: direct J/K build of the (H2O)32 / cc-pVDZ cluster on B200.
+"""Benchmark: direct J/K builds of an RHF SCF on the (H2O)32 / cc-pVDZ cluster.
 
-One step = one complete J/K build (density transform, every class-pair
-kernel, J/K finalisation) of the 768-function (H2O)32 cc-pVDZ cluster
-(seeded generator, seed 1), Schwarz cut 1e-12, one RHF-like density
-D = 2 C C^T (C ~ N(0,1)/sqrt(n), 5 occupied orbitals per water, seed 1).
+Workload: the 768-function (H2O)32 cc-pVDZ cluster from the seeded
+generator (seed 1), Schwarz cut 1e-12.  RHF from the core guess with DIIS;
+each iteration builds J/K incrementally from dD = D - D_last as the
+reference's SCF caller does (src/gradscf/scf/rks.py:305-321).
 
-Headline `value`: ERI quartets/s of the split-precision build (FP32 for
-quartets with Q_ij Q_kl max|D| < 1e-6), whole job over all ranks, inputs
-resident in HBM.  Quartets = significant canonical contracted shell quartets
-of the reference's shells (i>=j, k>=l, ij>=kl, Q_ij Q_kl >= 1e-12).  The
-FP64 build is measured in the same run (`fp64` key).  L2 is flushed (512 MB
-write) before every timed step; each step is timed with CUDA events on the
-launching stream.
+One step = one SCF iteration's complete J/K build (density transform, every
+class-pair kernel, finalisation).  Per precision mode the SCF runs
+exactly W + K iterations: W untimed, then K timed builds (CUDA events on the
+launching stream; L2 flushed by a 512 MB write before each).  FP64 mode
+evaluates every quartet in FP64; split mode evaluates quartets with
+Q_ij Q_kl max|dD| < 1e-6 in FP32 (FP64 accumulation).  The energy
+difference between the two runs after the same iterations is reported.
+
+Headline `value`: ERI quartets/s of the split-precision builds (whole job over
+all ranks).  Quartets = significant canonical contracted shell quartets of the
+reference's shells (i>=j, k>=l, ij>=kl, Q_ij Q_kl >= 1e-12) -- every build
+evaluates all of them.  `e2e` replays the K timed split builds through the
+public API with the dD copied from pinned host memory and J/K copied back.
 
 `--impl reference` times the reference's CPU path: libcint 6.1.3 compiled
 from the reference's sources, driven by the C restatement of its direct J/K
 driver (oracle/_ref), with all host threads, one full J/K build of the
 first 8 waters of the same cluster per step.
 
-Multi-GPU (torchrun): each rank builds J/K for its own replica of the
-workload (weak scaling, no collective on the data path); time = max over ranks.
+Multi-GPU (torchrun): each rank runs its own replica of the workload (weak
+scaling, no collective on the data path); times are the max over ranks.
 """
 from __future__ import annotations
 
@@ -40,16 +46,6 @@ METRIC = "J/K build s/iter & ERI quartets/s: split vs FP64 on B200 at |ΔE|≤1e
 WORKLOAD = "(H2O)32 cc-pVDZ direct J/K (768 sph AOs), Schwarz 1e-12, seed 1"
 FP32_CUT = 1e-6
 SAMPLE_WATERS = 8
-
-
-def build_workload(nwater=32, seed=1, basis="cc-pvdz"):
-    from gradscf_b200 import basis as B, workloads as W
-    spec = W.water_cluster(nwater, seed)
-    top, par, _ = B.prepare_basis(spec, basis, cart=False)
-    atm, bas, env = B.pack(top, par)
-    c = np.random.default_rng(seed).normal(size=(top.nao, 5 * nwater)) / np.sqrt(top.nao)
-    d = 2.0 * c @ c.T
-    return top, atm, bas, env, d
 
 
 def sample_workload():
@@ -140,7 +136,7 @@ class ClockSampler:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=12)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--nwater", type=int, default=32,
@@ -170,8 +166,7 @@ def main():
         return 0
 
     import torch
-    from gradscf_b200 import _capi, flop_model
-    from gradscf_b200.jk import DirectJKPlan
+    from gradscf_b200 import _capi, flop_model, scf, workloads
     import ctypes
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -185,92 +180,87 @@ def main():
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
     lib = _capi.lib()
+    st_h = ctypes.c_void_p(stream.cuda_stream)
 
-    top, atm, bas, env, dnp = build_workload(args.nwater)
-    plan = DirectJKPlan([(atm, bas, env)], cart=False, cutoff=1e-12, device=dev)
-    n = top.nao
-    d = torch.as_tensor(dnp.reshape(1, n * n), device=dev)
-    out = torch.empty((2, 1, n * n), dtype=torch.float64, device=dev)
+    spec = workloads.water_cluster(args.nwater, 1)
+    mol = scf.Molecule(spec, "cc-pvdz", cart=False, schwarz_cut=1e-12, device=dev)
+    atoms = spec.split("; ")
+    frags = ["; ".join(atoms[3 * i:3 * i + 3]) for i in range(args.nwater)]
+    d0 = scf.fragment_guess(mol, frags, "cc-pvdz")
+    plan = mol.plan
+    n = mol.nao
+    quartets = plan.quartets
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     peaks = {}
     for name, flag in (("fp64", 1), ("fp32", 0)):
         v = ctypes.c_double()
-        _capi.check(lib.b200jk_measure_fma_peak(flag, ctypes.byref(v), ctypes.c_void_p(stream.cuda_stream)))
+        _capi.check(lib.b200jk_measure_fma_peak(flag, ctypes.byref(v), st_h))
         peaks[name] = v.value
 
-    def step(precision):
-        plan.jk_packed(d, hermi=1, precision=precision, fp32_cut=FP32_CUT, out=out, check=False)
-
-    for _ in range(args.warmup):
-        step("fp64")
-        step("split")
-    _capi.check(lib.b200jk_check_status(plan._h, ctypes.c_void_p(stream.cuda_stream)))
-    torch.cuda.synchronize()
-
-    def energy(o):
-        j = o[0, 0].reshape(n, n)
-        k = o[1, 0].reshape(n, n)
-        dd = d[0].reshape(n, n)
-        return (0.5 * torch.sum(dd * j) - 0.25 * torch.sum(dd * k)).item()
-
-    step("fp64")
-    ref_out = out.clone()
-    e64 = energy(ref_out)
-    step("split")
-    e32 = energy(out)
-    max_dj = (out[0] - ref_out[0]).abs().max().item()
-    max_dk = (out[1] - ref_out[1]).abs().max().item()
-
     nc = _capi.NCLASS
+    classes = _capi.QUARTET_CLASSES
     q = (ctypes.c_int64 * nc)(); pq = (ctypes.c_int64 * nc)()
     _capi.check(lib.b200jk_plan_class_stats(plan._h, q, pq))
-    q64 = (ctypes.c_int64 * nc)(); q32 = (ctypes.c_int64 * nc)()
-    pq64 = (ctypes.c_int64 * nc)(); pq32 = (ctypes.c_int64 * nc)()
-    _capi.check(lib.b200jk_plan_split_stats(plan._h, ctypes.c_void_p(stream.cuda_stream), q64, q32, pq64, pq32))
     nclasspairs = sum(1 for c in range(nc) if q[c] > 0)
+    W, K = args.warmup, args.steps
+    total = W + K
 
-    results = {}
+    results, deltas_split = {}, []
     clocks = ClockSampler(local)
     with clocks:
         for precision in ("fp64", "split"):
-            if dist:
-                dist.barrier()
+            acc = {"q64": np.zeros(nc), "q32": np.zeros(nc), "pq64": np.zeros(nc), "pq32": np.zeros(nc),
+                   "maxdd": []}
+
+            def read_split_stats():
+                a_ = [(ctypes.c_int64 * nc)() for _ in range(4)]
+                _capi.check(lib.b200jk_plan_split_stats(plan._h, st_h, *a_))
+                for key, arr in zip(("q64", "q32", "pq64", "pq32"), a_):
+                    acc[key] += np.frombuffer(arr, dtype=np.int64)
+
+            def on_jk(cycle, delta, precision=precision):
+                if cycle - 1 > W and precision == "split":
+                    read_split_stats()          # stats of the previous (timed) build
+                if cycle > W:
+                    if cycle == W + 1:
+                        if dist:
+                            dist.barrier()
+                        torch.cuda.synchronize()
+                        lib.b200jk_plan_set_profiling(plan._h, 1)
+                    acc["maxdd"].append(delta.abs().max().item())
+                    if precision == "split":
+                        deltas_split.append(delta.detach().to("cpu").pin_memory())
+                    flush.zero_()
+
+            res = scf.rhf(mol, precision=precision, fp32_cut=FP32_CUT, fixed_cycles=total, on_jk=on_jk,
+                          density0=d0)
             torch.cuda.synchronize()
-            lib.b200jk_plan_set_profiling(plan._h, 1)
-            times = []
-            for _ in range(args.steps):
-                flush.zero_()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                step(precision)
-                e1.record(stream)
-                times.append((e0, e1))
-            torch.cuda.synchronize()
+            if precision == "split":
+                read_split_stats()
             if dist:
                 dist.barrier()
             lib.b200jk_plan_set_profiling(plan._h, 0)
-            ms = [a.elapsed_time(b) for a, b in times]
             ms64 = (ctypes.c_double * nc)(); ms32 = (ctypes.c_double * nc)(); nl = (ctypes.c_int32 * nc)()
             _capi.check(lib.b200jk_plan_profile(plan._h, ms64, ms32, nl))
-            step_ms = float(np.mean(ms))
+            step_ms = float(np.mean(res.jk_ms[W:]))
             if dist:
                 t = torch.tensor([step_ms], device=dev)
                 dist.all_reduce(t, op=dist.ReduceOp.MAX)
                 step_ms = t.item()
-            results[precision] = {"ms": step_ms, "ms64": list(ms64), "ms32": list(ms32),
-                                  "launches": list(nl)}
-        # end-to-end through the public API with pinned host buffers
+            results[precision] = {"ms": step_ms, "ms64": list(ms64), "ms32": list(ms32), "res": res,
+                                  "acc": acc}
+        # end-to-end through the public API: host dD in, host J/K out, every step
         hd = torch.empty((1, n * n), dtype=torch.float64, pin_memory=True)
-        hd.copy_(d.cpu())
         hout = torch.empty((2, 1, n * n), dtype=torch.float64, pin_memory=True)
-        dd = torch.empty_like(d)
-        e2e_ms = []
+        dd = torch.empty((1, n * n), dtype=torch.float64, device=dev)
+        out = torch.empty((2, 1, n * n), dtype=torch.float64, device=dev)
+        e2e = []
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        for _ in range(args.steps):
+        for delta in deltas_split:
+            hd.copy_(delta.reshape(1, n * n))
             flush.zero_()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -279,71 +269,66 @@ def main():
             plan.jk_packed(dd, hermi=1, precision="split", fp32_cut=FP32_CUT, out=out, check=False)
             hout.copy_(out, non_blocking=True)
             e1.record(stream)
-            e2e_ms.append((e0, e1))
+            e2e.append((e0, e1))
         torch.cuda.synchronize()
-        e2e_step = float(np.mean([a.elapsed_time(b) for a, b in e2e_ms]))
+        e2e_step = float(np.mean([a.elapsed_time(b) for a, b in e2e]))
         if dist:
             t = torch.tensor([e2e_step], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_step = t.item()
 
-    quartets = plan.quartets
-    qps = {p: world * quartets / (results[p]["ms"] * 1e-3) for p in results}
+    qps = {p_: world * quartets / (results[p_]["ms"] * 1e-3) for p_ in results}
+    r64, r32 = results["fp64"]["res"], results["split"]["res"]
+    acc = results["split"]["acc"]
 
-    # roofline of the dominant kernel of the split step
-    classes = _capi.QUARTET_CLASSES
-    best = None
+    # roofline of the dominant kernel over the timed split builds
+    best, top = None, []
     for c in range(nc):
-        for kind, msk, pqk, qk, peak in (("fp64", "ms64", pq64, q64, peaks["fp64"]),
-                                         ("fp32", "ms32", pq32, q32, peaks["fp32"])):
+        for kind, msk, pqk, qk, peak in (("fp64", "ms64", "pq64", "q64", peaks["fp64"]),
+                                         ("fp32", "ms32", "pq32", "q32", peaks["fp32"])):
             t = results["split"][msk][c]
-            if t > 0 and (best is None or t > best[0]):
-                flops = flop_model.class_flops(classes[c], pqk[c], qk[c])
-                best = (t, c, kind, flops, peak)
+            if t <= 0:
+                continue
+            fl = flop_model.class_flops(classes[c], acc[pqk][c], acc[qk][c])
+            top.append({"class": "(%d%d|%d%d)" % classes[c], "prec": kind, "ms_per_step": round(t / K, 3),
+                        "tflops": round(fl / (t * 1e-3) / 1e12, 3) if fl else 0.0})
+            if best is None or t > best[0]:
+                best = (t, c, kind, fl, peak)
+    top.sort(key=lambda r: -r["ms_per_step"])
     t_ms, c, kind, flops, peak = best
-    launches = results["split"]["launches"][c] / 2 / args.steps  # fp64+fp32 share the count
-    per_launch_ms = t_ms / args.steps
-    achieved = flops / (per_launch_ms * 1e-3) / 1e12
+    achieved = flops / (t_ms * 1e-3) / 1e12
     total_ms = sum(results["split"]["ms64"]) + sum(results["split"]["ms32"])
     roofline = {"bound": kind, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": None,
-                "kernel": f"class ({classes[c][0]}{classes[c][1]}|{classes[c][2]}{classes[c][3]}) {kind}",
+                "kernel": f"jk class ({classes[c][0]}{classes[c][1]}|{classes[c][2]}{classes[c][3]}) {kind}",
                 "share_of_step": t_ms / total_ms,
                 "peak_source": f"measured {kind} FMA microkernel on this GPU (b200jk_measure_fma_peak)"}
-    # whole-build FLOP rate in FP64 mode (all classes)
-    fl64 = sum(flop_model.class_flops(classes[c], pq[c], q[c]) for c in range(nc))
+    fl64 = sum(flop_model.class_flops(classes[c_], pq[c_], q[c_]) for c_ in range(nc))
     fp64_build = {"ms_per_build": results["fp64"]["ms"], "quartets_per_s": qps["fp64"],
                   "model_tflops": fl64 / (results["fp64"]["ms"] * 1e-3) / 1e12,
                   "frac_of_fp64_peak": fl64 / (results["fp64"]["ms"] * 1e-3) / 1e12 / peaks["fp64"]}
-
-    top = []
-    for c in range(nc):
-        for kind, msk, pqk, qk in (("fp64", "ms64", pq64, q64), ("fp32", "ms32", pq32, q32)):
-            t = results["split"][msk][c] / args.steps
-            if t > 0:
-                fl = flop_model.class_flops(classes[c], pqk[c], qk[c])
-                top.append({"class": "(%d%d|%d%d)" % classes[c], "prec": kind, "ms": round(t, 3),
-                            "quartets": int(qk[c]), "prim_quartets": int(pqk[c]),
-                            "tflops": round(fl / (t * 1e-3) / 1e12, 3)})
-    top.sort(key=lambda r: -r["ms"])
-    gpu_launches = args.steps * (2 + 1 + nclasspairs + 2 * nclasspairs)
+    gpu_launches = K * (2 + 1 + 1 + nclasspairs + 2 * nclasspairs)
     line = {"metric": METRIC, "value": qps["split"], "unit": "quartets/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": results["split"]["ms"],
+            "steps": K, "warmup": W, "ms_per_step": results["split"]["ms"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32/f64 split (f64 accumulation)", "data": "synthetic",
             "config": {"workload": WORKLOAD if args.nwater == 32 else f"(H2O){args.nwater} cc-pVDZ (profiling case)",
-                       "quartets": quartets, "nao": n,
-                       "fp32_cut": FP32_CUT, "density": "2 C C^T, C~N(0,1)/sqrt(n), 160 occ, seed 1",
-                       "l2": "flushed (512 MB write) before every timed step",
+                       "step": "one RHF iteration's incremental J/K build (dD = D - D_last)",
+                       "scf": f"fragment guess (converged monomer densities), DIIS(8), {W} untimed + {K} timed iterations per mode",
+                       "quartets_per_build": quartets, "nao": n, "fp32_cut": FP32_CUT,
+                       "l2": "flushed (512 MB write) before every timed build",
                        "parallelism": f"replicas x{world}"},
+            "s_per_iter": {"split": results["split"]["ms"] * 1e-3, "fp64": results["fp64"]["ms"] * 1e-3},
             "fp64": fp64_build,
             "split_speedup_vs_fp64": results["fp64"]["ms"] / results["split"]["ms"],
-            "split_error": {"max_abs_dJ": max_dj, "max_abs_dK": max_dk,
-                            "dE_2e_hartree": abs(e32 - e64)},
-            "split_fraction_fp32_quartets": sum(q32) / max(1, sum(q32) + sum(q64)),
+            "energy": {"fp64_hartree": r64.energy, "split_hartree": r32.energy,
+                       "abs_dE_hartree": abs(r32.energy - r64.energy),
+                       "last_iter_dE_fp64": abs(r64.energies[-1] - r64.energies[-2])},
+            "split_fraction_fp32_quartets": float(acc["q32"].sum() / max(1.0, acc["q32"].sum() + acc["q64"].sum())),
+            "max_abs_dD_timed": [float(x) for x in acc["maxdd"]],
             "e2e": {"value": world * quartets / (e2e_step * 1e-3), "unit": "quartets/s",
-                    "ms_per_step": e2e_step, "h2d_bytes_per_step": int(d.numel() * 8),
-                    "d2h_bytes_per_step": int(out.numel() * 8)},
+                    "ms_per_step": e2e_step, "h2d_bytes_per_step": int(n * n * 8),
+                    "d2h_bytes_per_step": int(2 * n * n * 8)},
             "roofline": roofline, "gpu_launches": gpu_launches, "clocks": clocks.summary(),
             "top_kernels_split_step": top[:8]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -65,6 +65,11 @@ struct Tables {
   const double* boys;       // [row][col] F_col(row / BOYS_STEP_INV)
   const float* boys_f;
   const double* c2s;        // per l: [kTW][kTW] output transform (cart->sph or cart factor)
+  // Per-order Taylor tables for the closed-form roots: for M = 1, 3, 5 (table
+  // (M-1)/2), row k holds F_{M+i}(k/20) / i!, i = 0..7 -- one aligned 64-byte
+  // (double) / 32-byte (float) row per lookup.
+  const double* boys_m;
+  const float* boys_m_f;
 };
 
 // Output-transform table layout: per l a kTW x kTW block, row = raw Cartesian
@@ -72,9 +77,9 @@ struct Tables {
 constexpr int kTW = 10;
 constexpr int kTS = kTW * kTW;
 
-// Boys function F_0..F_M(T) into f[0..M], M <= 8.
-// T < 40: 8-term Taylor expansion of F_M about the nearest grid point
-// (spacing 1/20) followed by the stable downward recursion
+// Boys function F_0..F_M(T) into f[0..M], M in {1, 3, 5}.
+// T < 40: Taylor expansion of F_M about the nearest grid point (spacing
+// 1/20; 8 terms in FP64, 5 in FP32) followed by the stable downward recursion
 //   F_m = (2 T F_{m+1} + e^{-T}) / (2m + 1).
 // T >= 40: F_0 = sqrt(pi/T)/2 and the stable upward recursion
 //   F_{m+1} = ((2m+1) F_m - e^{-T}) / (2T).
@@ -82,21 +87,31 @@ constexpr int kTS = kTW * kTW;
 // Division-free: constant divisors are multiplications by folded reciprocals.
 template <int M, typename R>
 __device__ __forceinline__ void boys_fn(R t, R* f, const R* grid) {
-  constexpr int NCOL = 24;       // BOYS_MMAX + BOYS_TERMS
+  static_assert(M == 1 || M == 3 || M == 5, "per-order tables exist for M = 1, 3, 5");
   if (t < R(40)) {
     const int k = min(max(__float2int_rn(float(t) * 20.0f), 0), 800);
     const R dt = R(k) * R(0.05) - t;          // -(t - t_k)
-    const R* row = grid + k * NCOL + M;
-    R acc = row[7];
-#pragma unroll
-    for (int i = 6; i >= 0; --i) acc = row[i] + acc * (dt * R(1.0 / (i + 1)));
-    f[M] = acc;
-    if (M > 0) {
-      const R e = dexp<R>(-t);
-      const R t2 = t + t;
-#pragma unroll
-      for (int m = M - 1; m >= 0; --m) f[m] = (t2 * f[m + 1] + e) * R(1.0 / (2 * m + 1));
+    const R* row = grid + ((M - 1) / 2 * 801 + k) * 8;
+    R c[8];
+    if constexpr (sizeof(R) == 8) {
+      const double4 a = reinterpret_cast<const double4*>(row)[0];
+      const double4 b = reinterpret_cast<const double4*>(row)[1];
+      c[0] = a.x; c[1] = a.y; c[2] = a.z; c[3] = a.w; c[4] = b.x; c[5] = b.y; c[6] = b.z; c[7] = b.w;
+    } else {
+      const float4 a = reinterpret_cast<const float4*>(row)[0];
+      const float4 b = reinterpret_cast<const float4*>(row)[1];
+      c[0] = a.x; c[1] = a.y; c[2] = a.z; c[3] = a.w; c[4] = b.x; c[5] = b.y; c[6] = b.z; c[7] = b.w;
     }
+    // FP32 needs 5 terms (|dt| <= 0.025: truncation ~1e-10), FP64 all 8
+    constexpr int NT = sizeof(R) == 8 ? 8 : 5;
+    R acc = c[NT - 1];
+#pragma unroll
+    for (int i = NT - 2; i >= 0; --i) acc = c[i] + acc * dt;
+    f[M] = acc;
+    const R e = dexp<R>(-t);
+    const R t2 = t + t;
+#pragma unroll
+    for (int m = M - 1; m >= 0; --m) f[m] = (t2 * f[m + 1] + e) * R(1.0 / (2 * m + 1));
   } else {
     const R e = dexp<R>(-t);
     const R rs = drsqrt<R>(t);
@@ -211,11 +226,11 @@ __device__ __forceinline__ R rys_cheb(const R* tab, int off, int nfun, int fidx,
 template <typename R> struct TableSel;
 template <> struct TableSel<double> {
   static __device__ __forceinline__ const double* rys(const Tables& t) { return t.rys; }
-  static __device__ __forceinline__ const double* boys(const Tables& t) { return t.boys; }
+  static __device__ __forceinline__ const double* boys(const Tables& t) { return t.boys_m; }
 };
 template <> struct TableSel<float> {
   static __device__ __forceinline__ const float* rys(const Tables& t) { return t.rys_f; }
-  static __device__ __forceinline__ const float* boys(const Tables& t) { return t.boys_f; }
+  static __device__ __forceinline__ const float* boys(const Tables& t) { return t.boys_m_f; }
 };
 
 // All N nodes/weights by one thread: closed forms for N <= 3, the

@@ -92,7 +92,7 @@ static void output_transform(int l, int cart, double* t /* [10][10] */) {
 // ---------------------------------------------------------------- tables
 struct DeviceTables {
   Tables t{};
-  DevBuf rys, rys_f, off, nint, ar, aw, boys, boys_f, c2s_sph, c2s_cart;
+  DevBuf rys, rys_f, off, nint, ar, aw, boys, boys_f, c2s_sph, c2s_cart, boys_m, boys_m_f;
   Tables sph, cartt;
 };
 
@@ -118,6 +118,21 @@ static DeviceTables& tables_for(int device) {
   up(d->boys, kBoysGrid, sizeof(kBoysGrid));
   std::vector<float> bf(kBoysGrid, kBoysGrid + BOYS_NROW * BOYS_NCOL);
   up(d->boys_f, bf.data(), bf.size() * sizeof(float));
+  {
+    // per-order Taylor rows: F_{M+i}(k/20) / i!, M = 1, 3, 5
+    std::vector<double> bm(3 * 801 * 8);
+    for (int mi = 0; mi < 3; ++mi)
+      for (int k = 0; k < 801; ++k) {
+        double fact_i = 1.0;
+        for (int i = 0; i < 8; ++i) {
+          if (i > 0) fact_i *= i;
+          bm[(mi * 801 + k) * 8 + i] = kBoysGrid[k * BOYS_NCOL + (2 * mi + 1) + i] / fact_i;
+        }
+      }
+    up(d->boys_m, bm.data(), bm.size() * sizeof(double));
+    std::vector<float> bmf(bm.begin(), bm.end());
+    up(d->boys_m_f, bmf.data(), bmf.size() * sizeof(float));
+  }
   std::vector<double> cs(4 * kTS), cc(4 * kTS);
   for (int l = 0; l <= 3; ++l) {
     output_transform(l, 0, cs.data() + l * kTS);
@@ -134,6 +149,8 @@ static DeviceTables& tables_for(int device) {
   base.asym_w = d->aw.as<double>();
   base.boys = d->boys.as<double>();
   base.boys_f = d->boys_f.as<float>();
+  base.boys_m = d->boys_m.as<double>();
+  base.boys_m_f = d->boys_m_f.as<float>();
   d->sph = base;
   d->sph.c2s = d->c2s_sph.as<double>();
   d->cartt = base;

@@ -197,12 +197,14 @@ __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const Quar
   constexpr int N = CI::NROOT;
 #pragma unroll
   for (int o = 0; o < CI::NOUT; ++o) out[o] = R(0);
-  for (int i = 0; i < g.npa; ++i) {
-    const double4 P = bpp[i];
-    const double2 PA = baux[i];
-    for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
+  // ket primitive in registers (outer), bra primitives broadcast from
+  // shared memory (inner): one global read per ket primitive pair.
+  for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
+    const double4 Q = args.pp_data[j];
+    const double2 QA = args.pp_aux[j];
+    for (int i = 0; i < g.npa; ++i) {
       PrimQ<R> s;
-      prim_setup<R>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
+      prim_setup<R>(g, bpp[i], baux[i], Q, QA, s);
       R x[N], w[N];
       rys_roots<N, R>(s.t, x, w, args.tb);
 #pragma unroll

@@ -73,8 +73,14 @@ def _solve(f, x):
 
 
 def rhf(mol: Molecule, *, conv_tol=1e-10, conv_tol_grad=None, max_cycle=100, precision="fp64",
-        fp32_cut=DEFAULT_FP32_CUT, incremental=True, diis_space=8, density0=None, timing=True):
-    """Run RHF; returns SCFResult (energy in Hartree)."""
+        fp32_cut=DEFAULT_FP32_CUT, incremental=True, diis_space=8, density0=None, timing=True,
+        fixed_cycles=None, on_jk=None):
+    """Run RHF; returns SCFResult (energy in Hartree).
+
+    fixed_cycles: run exactly that many iterations (no convergence stop).
+    on_jk(cycle, delta): optional callback before each J/K build (e.g. to
+    flush L2 or toggle profiling); its work is outside the timed build.
+    """
     dev = mol.device
     s = mol.int1e("ovlp")
     h = mol.int1e("kin") + mol.int1e("nuc")
@@ -96,8 +102,11 @@ def rhf(mol: Molecule, *, conv_tol=1e-10, conv_tol_grad=None, max_cycle=100, pre
     energies, jk_ms = [], []
     converged = False
     stream = torch.cuda.current_stream(dev)
-    for cycle in range(1, max_cycle + 1):
+    ncyc = fixed_cycles if fixed_cycles is not None else max_cycle
+    for cycle in range(1, ncyc + 1):
         delta = d - d_last if incremental else d
+        if on_jk is not None:
+            on_jk(cycle, delta)
         if timing:
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ev0.record(stream)
@@ -118,7 +127,8 @@ def rhf(mol: Molecule, *, conv_tol=1e-10, conv_tol_grad=None, max_cycle=100, pre
         gnorm = torch.linalg.norm(err_o).item()
         if e_old is not None and abs(energy - e_old) < conv_tol and gnorm < conv_tol_grad:
             converged = True
-            break
+            if fixed_cycles is None:
+                break
         hist_f.append(f)
         hist_e.append(err_o)
         hist_f, hist_e = hist_f[-diis_space:], hist_e[-diis_space:]
@@ -177,3 +187,128 @@ def rhf_gradient(mol: Molecule, res: SCFResult):
     for s, a in enumerate(mol.shell_atoms):
         out[a] += g[mol.bas[s, 0]]
     return out + nuclear_repulsion_gradient(mol.charges, mol.coords)
+
+
+class MoleculeBatch:
+    """Independent molecules sharing one device plan (packed per-molecule blocks)."""
+
+    def __init__(self, atoms, basis, *, unit="Angstrom", cart=False, schwarz_cut=1e-12, device=None):
+        self.mols = []
+        tables = []
+        for atom in atoms:
+            top, par, sa = prepare_basis(atom, basis, unit=unit, cart=cart)
+            atm, bas, env = pack(top, par)
+            charges = np.asarray(top.nuclear_charges, dtype=np.float64)
+            coords = np.asarray(par.nuclear_coords, dtype=np.float64)
+            self.mols.append(dict(atm=atm, bas=bas, env=env, charges=charges, coords=coords,
+                                  nelectron=int(charges.sum()), e_nuc=nuclear_repulsion(charges, coords)))
+            tables.append((atm, bas, env))
+        self.plan = DirectJKPlan(tables, cart=cart, cutoff=schwarz_cut, device=device)
+        self.device = self.plan.device
+        self.nao = self.plan.nao
+        self.offsets = self.plan.offsets
+
+    def int1e(self, which):
+        out = torch.empty((self.plan.packed_size,), dtype=torch.float64, device=self.device)
+        code = {"ovlp": 0, "kin": 1, "nuc": 2}[which]
+        with torch.cuda.device(self.device):
+            st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+            _capi.check(_capi.lib().b200jk_int1e(self.plan._h, code, ctypes.c_void_p(out.data_ptr()), st))
+        return out
+
+    def block(self, packed, m):
+        n = self.nao[m]
+        return packed[self.offsets[m]:self.offsets[m] + n * n].view(n, n)
+
+
+def rhf_batch(batch: MoleculeBatch, *, conv_tol=1e-10, max_cycle=60, precision="fp64",
+              fp32_cut=DEFAULT_FP32_CUT, diis_space=8, timing=True):
+    """RHF of every molecule of the batch; one packed J/K build per iteration
+    serves all molecules.  Returns (energies, densities, jk_ms, cycles, converged)."""
+    dev = batch.device
+    s_all, h_all = batch.int1e("ovlp"), batch.int1e("kin") + batch.int1e("nuc")
+    nm = len(batch.mols)
+    xs, ds, hs, ss = [], [], [], []
+    for m in range(nm):
+        s = batch.block(s_all, m)
+        h = batch.block(h_all, m)
+        w, v = torch.linalg.eigh(s)
+        x = v / torch.sqrt(w)
+        e, c = _solve(h, x)
+        nocc = batch.mols[m]["nelectron"] // 2
+        xs.append(x); hs.append(h); ss.append(s)
+        ds.append(2.0 * c[:, :nocc] @ c[:, :nocc].T)
+    d_last = torch.zeros((batch.plan.packed_size,), dtype=torch.float64, device=dev)
+    jk = torch.zeros((2, batch.plan.packed_size), dtype=torch.float64, device=dev)
+    hist = [([], []) for _ in range(nm)]
+    e_old = [None] * nm
+    done = [False] * nm
+    energies = [0.0] * nm
+    jk_ms = []
+    stream = torch.cuda.current_stream(dev)
+    conv_tol_grad = float(np.sqrt(conv_tol))
+    cycle = 0
+    for cycle in range(1, max_cycle + 1):
+        d_packed = torch.cat([d.reshape(-1) for d in ds])
+        delta = (d_packed - d_last).reshape(1, -1).contiguous()
+        if timing:
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+        out = batch.plan.jk_packed(delta, hermi=1, precision=precision, fp32_cut=fp32_cut)
+        if timing:
+            ev1.record(stream)
+            jk_ms.append((ev0, ev1))
+        jk += out[:, 0]
+        d_last = d_packed
+        for m in range(nm):
+            if done[m]:
+                continue
+            d, h, s, x = ds[m], hs[m], ss[m], xs[m]
+            j, k = batch.block(jk[0], m), batch.block(jk[1], m)
+            f = h + j - 0.5 * k
+            en = (torch.sum(d * h) + 0.5 * torch.sum(d * j) - 0.25 * torch.sum(d * k)).item() + batch.mols[m]["e_nuc"]
+            energies[m] = en
+            err_o = x.T @ (f @ d @ s - s @ d @ f) @ x
+            if e_old[m] is not None and abs(en - e_old[m]) < conv_tol and torch.linalg.norm(err_o).item() < conv_tol_grad:
+                done[m] = True
+                continue
+            hf, he = hist[m]
+            hf.append(f); he.append(err_o)
+            del hf[:-diis_space], he[:-diis_space]
+            if len(hf) > 1:
+                k_ = len(hf)
+                b = -torch.ones((k_ + 1, k_ + 1), dtype=torch.float64, device=dev)
+                b[k_, k_] = 0.0
+                for a in range(k_):
+                    for c_ in range(a, k_):
+                        b[a, c_] = b[c_, a] = torch.sum(he[a] * he[c_])
+                rhs = torch.zeros(k_ + 1, dtype=torch.float64, device=dev)
+                rhs[k_] = -1.0
+                coef = torch.linalg.solve(b, rhs)[:k_]
+                f = sum(cf * fi for cf, fi in zip(coef, hf))
+            e, c = _solve(f, x)
+            nocc = batch.mols[m]["nelectron"] // 2
+            ds[m] = 2.0 * c[:, :nocc] @ c[:, :nocc].T
+            e_old[m] = en
+        if all(done):
+            break
+    torch.cuda.synchronize(dev)
+    times = [a.elapsed_time(b) for a, b in jk_ms] if timing else []
+    return energies, ds, times, cycle, done
+
+
+def fragment_guess(mol: Molecule, fragments, basis, *, unit="Angstrom"):
+    """Block-diagonal guess density from converged RHF densities of the
+    fragments (consecutive atoms of `mol`, in order), all solved in one
+    batched J/K plan."""
+    batch = MoleculeBatch(fragments, basis, unit=unit, cart=mol.cart, device=mol.device)
+    _, ds, _, _, _ = rhf_batch(batch, conv_tol=1e-8, timing=False)
+    d0 = torch.zeros((mol.nao, mol.nao), dtype=torch.float64, device=mol.device)
+    o = 0
+    for d in ds:
+        n = d.shape[0]
+        d0[o:o + n, o:o + n] = d
+        o += n
+    if o != mol.nao:
+        raise ValueError("fragments do not cover the molecule's basis")
+    return d0
