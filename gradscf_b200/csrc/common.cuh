@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #define B200JK_PI 3.14159265358979323846
 // 2 pi^(5/2): prefactor of the (ss|ss) integral, 2 pi^2.5 / (p q sqrt(p+q)).
 #define B200JK_ERI_C0 34.98683665524972497
@@ -26,6 +28,17 @@ __host__ __device__ constexpr int cart_ly(int l, int i) {
 }
 __host__ __device__ constexpr int cart_lz(int l, int i) {
   return l - cart_lx(l, i) - cart_ly(l, i);
+}
+
+// Compile-time loop: f(std::integral_constant<int, I>) for I in [B, E), so
+// indices derived from I are constant expressions (register arrays stay in
+// registers).
+template <int B, int E, typename F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (B < E) {
+    f(std::integral_constant<int, B>{});
+    static_for<B + 1, E>(f);
+  }
 }
 
 template <int LA, int LB, int LC, int LD>
@@ -189,7 +202,7 @@ __device__ __forceinline__ void rys_small(R t, R* x, R* w, const R* grid) {
     R lam[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      R l = R(2.0f * r * cosf(th - 2.0943951023931955f * float(k))) + m;
+      R l = R(2.0f * r * __cosf(th - 2.0943951023931955f * float(k))) + m;   // polished below
       const R dpi = R(1.0f / float((R(3) * l + R(2) * c2) * l + c1));
 #pragma unroll
       for (int it = 0; it < 2; ++it) l -= (((l + c2) * l + c1) * l + c0) * dpi;

@@ -403,6 +403,8 @@ static JKArgs base_args(const Plan& p) {
   a.pp_data = p.d_pp_data.as<double4>();
   a.pp_aux = p.d_pp_aux.as<double2>();
   a.pp_exp = p.d_pp_exp.as<double2>();
+  a.pp_f = p.d_pp_f.as<float4>();
+  a.pp_f2 = p.d_pp_f2.as<float2>();
   a.ws_atm = p.d_ws_atm.as<int>();
   a.mol_base = p.d_mol_base_cart.as<long long>();
   a.mol_n = p.d_mol_ncart.as<int>();
@@ -474,6 +476,8 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
   // ---- shell pairs and primitive pairs
   std::vector<double4> pp_data;
   std::vector<double2> pp_aux, pp_exp;
+  std::vector<float4> pp_f;
+  std::vector<float2> pp_f2;
   int ws0 = 0;
   for (int m = 0; m < nmol; ++m) {
     int wsn = ws0;
@@ -497,6 +501,9 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
                                            (a * ra.z + b * rb.z) / pe, pe));
             pp_aux.push_back(make_double2(std::exp(-expo) * ca * cbv / pe, 0.5 / pe));
             pp_exp.push_back(make_double2(a, b));
+            pp_f.push_back(make_float4(float(pp_data.back().x - ra.x), float(pp_data.back().y - ra.y),
+                                       float(pp_data.back().z - ra.z), float(pe)));
+            pp_f2.push_back(make_float2(float(pp_aux.back().x), float(0.5 / pe)));
           }
         const int cnt = (int)pp_data.size() - off;
         if (cnt == 0) continue;
@@ -513,6 +520,8 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
   upload(p.d_pp_data, pp_data.data(), pp_data.size() * sizeof(double4));
   upload(p.d_pp_aux, pp_aux.data(), pp_aux.size() * sizeof(double2));
   upload(p.d_pp_exp, pp_exp.data(), pp_exp.size() * sizeof(double2));
+  upload(p.d_pp_f, pp_f.data(), pp_f.size() * sizeof(float4));
+  upload(p.d_pp_f2, pp_f2.data(), pp_f2.size() * sizeof(float2));
   upload(p.d_mol_base_cart, p.mol_cart_base.data(), nmol * sizeof(long long));
   upload(p.d_mol_ncart, p.mol_ncart.data(), nmol * sizeof(int));
   upload(p.d_mol_base_out, p.mol_out_base.data(), nmol * sizeof(long long));
@@ -644,7 +653,7 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
       const ClassList& Y = p.classes[y];
       if (X.pairs.empty() || Y.pairs.empty()) continue;
       const int cls = quartet_class(x, y);
-      const int chunk = disp.reg_path[cls] ? 256 : std::max(8, 4 * (128 / disp.team[cls]));
+      const int chunk = disp.reg_path[cls] ? 64 : std::max(8, 4 * (128 / disp.team[cls]));
       auto* W = new ClassPairWork();
       W->x = x;
       W->y = y;

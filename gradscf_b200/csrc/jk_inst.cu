@@ -30,7 +30,7 @@ int launch_class(const JKArgs& args, cudaStream_t stream) {
   if (args.nwork <= 0) return 0;
   using P = Policy<LA, LB, LC, LD>;
   if constexpr (P::REG) {
-    jk_reg_kernel<LA, LB, LC, LD, R><<<args.nwork, 128, 0, stream>>>(args);
+    jk_reg_kernel<LA, LB, LC, LD, R><<<(args.nwork + kRegWarps - 1) / kRegWarps, 32 * kRegWarps, 0, stream>>>(args);
   } else {
     constexpr int TEAM = P::TEAM;
     using SM = TeamSmem<LA, LB, LC, LD, R, TEAM>;

@@ -26,6 +26,8 @@ struct JKArgs {
   const int4* pair_info;     // (shell A, shell B, first primitive pair, count)
   const double4* pp_data;    // primitive pair: (Px, Py, Pz, p = a+b)
   const double2* pp_aux;     // (exp(-ab/p |AB|^2) c_a c_b / p, 1/(2p))
+  const float4* pp_f;        // FP32 copy: (P - A, p)
+  const float2* pp_f2;       // FP32 copy: (K/p, 1/(2p))
   const long long* mol_base; // offset of the molecule's n x n block
   const int* mol_n;          // Cartesian AO count of the molecule
   const int* bra_pairs;      // sorted pair ids of the bra class
@@ -160,6 +162,51 @@ __device__ __forceinline__ void prim_setup(const QuartetGeom& g, const double4 P
   s.pqx = R(pqx); s.pqy = R(pqy); s.pqz = R(pqz);
 }
 
+// FP32 quartets: per-primitive data stored relative to the shell centre in
+// FP32, P - Q = (A - C) + (P - A) - (Q - C) with A - C formed once per quartet.
+__device__ __forceinline__ void prim_setup_f(const float3 ac, const float4 P, const float2 PA,
+                                             const float4 Q, const float2 QA, PrimQ<float>& s) {
+  const float p = P.w, q = Q.w;
+  const float pq = p + q;
+  const float rs = rsqrtf(pq);
+  const float ipq = rs * rs;
+  const float pqx = ac.x + P.x - Q.x, pqy = ac.y + P.y - Q.y, pqz = ac.z + P.z - Q.z;
+  s.t = p * q * ipq * (pqx * pqx + pqy * pqy + pqz * pqz);
+  s.pref = float(B200JK_ERI_C0) * PA.x * QA.x * rs;
+  s.pq_inv = ipq;
+  s.q_pq = q * ipq;
+  s.p_pq = p * ipq;
+  s.inv2p = PA.y;
+  s.inv2q = QA.y;
+  s.pax = P.x; s.pay = P.y; s.paz = P.z;
+  s.qcx = Q.x; s.qcy = Q.y; s.qcz = Q.z;
+  s.pqx = pqx; s.pqy = pqy; s.pqz = pqz;
+}
+
+// Primitive-pair storage type per precision (bra cache and ket reads).
+template <typename R> struct PrimData;
+template <> struct PrimData<double> {
+  using A = double4;
+  using B = double2;
+  static __device__ __forceinline__ A a(const JKArgs& x, int i) { return x.pp_data[i]; }
+  static __device__ __forceinline__ B b(const JKArgs& x, int i) { return x.pp_aux[i]; }
+};
+template <> struct PrimData<float> {
+  using A = float4;
+  using B = float2;
+  static __device__ __forceinline__ A a(const JKArgs& x, int i) { return x.pp_f[i]; }
+  static __device__ __forceinline__ B b(const JKArgs& x, int i) { return x.pp_f2[i]; }
+};
+
+template <typename R>
+__device__ __forceinline__ void prim_any(const QuartetGeom& g, const float3 ac,
+                                         const typename PrimData<R>::A P, const typename PrimData<R>::B PA,
+                                         const typename PrimData<R>::A Q, const typename PrimData<R>::B QA,
+                                         PrimQ<R>& s) {
+  if constexpr (sizeof(R) == 4) prim_setup_f(ac, P, PA, Q, QA, s);
+  else prim_setup<double>(g, P, PA, Q, QA, s);
+}
+
 // Rys coefficients of one root for the three axes.
 template <typename R>
 struct RootCoef {
@@ -191,7 +238,8 @@ __device__ __forceinline__ long long dm_index(const JKArgs& args, int mol, int a
 // ---------------------------------------------------------------------------
 template <int LA, int LB, int LC, int LD, typename R>
 __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const QuartetGeom& g,
-                                                  const double4* bpp, const double2* baux, R* out) {
+                                                  const typename PrimData<R>::A* bpp,
+                                                  const typename PrimData<R>::B* baux, R* out) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   using GI = GIdx<LA, LB, LC, LD>;
   constexpr int N = CI::NROOT;
@@ -199,12 +247,13 @@ __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const Quar
   for (int o = 0; o < CI::NOUT; ++o) out[o] = R(0);
   // ket primitive in registers (outer), bra primitives broadcast from
   // shared memory (inner): one global read per ket primitive pair.
+  const float3 ac = make_float3(float(g.ax - g.cx), float(g.ay - g.cy), float(g.az - g.cz));
   for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
-    const double4 Q = args.pp_data[j];
-    const double2 QA = args.pp_aux[j];
+    const auto Q = PrimData<R>::a(args, j);
+    const auto QA = PrimData<R>::b(args, j);
     for (int i = 0; i < g.npa; ++i) {
       PrimQ<R> s;
-      prim_setup<R>(g, bpp[i], baux[i], Q, QA, s);
+      prim_any<R>(g, ac, bpp[i], baux[i], Q, QA, s);
       R x[N], w[N];
       rys_roots<N, R>(s.t, x, w, args.tb);
 #pragma unroll
@@ -218,20 +267,15 @@ __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const Quar
                                    R(g.cdy), gy);
         build_g<LA, LB, LC, LD, R>(rc.c00[2], rc.c0p[2], rc.b10, rc.b01, rc.b00, w[r] * s.pref,
                                    R(g.abz), R(g.cdz), gz);
-#pragma unroll
-        for (int ia = 0; ia < CI::NA; ++ia)
-#pragma unroll
-          for (int ib = 0; ib < CI::NB; ++ib)
-#pragma unroll
-            for (int ic = 0; ic < CI::NC; ++ic)
-#pragma unroll
-              for (int id = 0; id < CI::ND; ++id) {
-                const int o = ((ia * CI::NB + ib) * CI::NC + ic) * CI::ND + id;
-                const int jx = GI::idx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
-                const int jy = GI::idx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
-                const int jz = GI::idx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
-                out[o] += gx[jx] * gy[jy] * gz[jz];
-              }
+        static_for<0, CI::NOUT>([&](auto O) {
+          constexpr int o = decltype(O)::value;
+          constexpr int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
+          constexpr int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
+          constexpr int jx = GI::idx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
+          constexpr int jy = GI::idx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
+          constexpr int jz = GI::idx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
+          out[o] += gx[jx] * gy[jy] * gz[jz];
+        });
       }
     }
   }
@@ -242,7 +286,7 @@ __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const Quar
 // elements are read where they are used (L1/L2 resident).
 template <int LA, int LB, int LC, int LD, typename R>
 __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom& g, const R* out,
-                                           bool acc_j, double* jab) {
+                                           bool acc_j, bool active, double* s_jab_row) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   constexpr int NA = CI::NA, NB = CI::NB, NC = CI::NC, ND = CI::ND;
   const double s = g.scale;
@@ -265,8 +309,15 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
           for (int c = 0; c < NC; ++c)
 #pragma unroll
             for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoC + c) * n + g.aoD + d);
-          if (acc_j && e == 0) jab[a * NB + b] = 2.0 * s * double(acc);
-          else atomicAdd(vj + (long long)(g.aoA + a) * n + g.aoB + b, 2.0 * s * double(acc));
+          if (acc_j && e == 0) {
+            // bra-block J of density 0: warp-reduced here, added once per work item
+            double v = active ? 2.0 * s * double(acc) : 0.0;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if ((threadIdx.x & 31) == 0) s_jab_row[a * NB + b] += v;
+          } else if (active) {
+            atomicAdd(vj + (long long)(g.aoA + a) * n + g.aoB + b, 2.0 * s * double(acc));
+          }
         }
 #pragma unroll
       for (int c = 0; c < NC; ++c)
@@ -277,7 +328,7 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
           for (int a = 0; a < NA; ++a)
 #pragma unroll
             for (int b = 0; b < NB; ++b) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoA + a) * n + g.aoB + b);
-          atomicAdd(vj + (long long)(g.aoC + c) * n + g.aoD + d, 2.0 * s * double(acc));
+          if (active) atomicAdd(vj + (long long)(g.aoC + c) * n + g.aoD + d, 2.0 * s * double(acc));
         }
     }
     if (args.with_k) {
@@ -291,7 +342,7 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
           for (int b = 0; b < NB; ++b)
 #pragma unroll
             for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoB + b) * n + g.aoD + d);
-          atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoC + c, s * double(acc));
+          if (active) atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoC + c, s * double(acc));
         }
 #pragma unroll
       for (int a = 0; a < NA; ++a)
@@ -302,7 +353,7 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
           for (int b = 0; b < NB; ++b)
 #pragma unroll
             for (int c = 0; c < NC; ++c) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoB + b) * n + g.aoC + c);
-          atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoD + d, s * double(acc));
+          if (active) atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoD + d, s * double(acc));
         }
 #pragma unroll
       for (int b = 0; b < NB; ++b)
@@ -313,7 +364,7 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
           for (int a = 0; a < NA; ++a)
 #pragma unroll
             for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoA + a) * n + g.aoD + d);
-          atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoC + c, s * double(acc));
+          if (active) atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoC + c, s * double(acc));
         }
 #pragma unroll
       for (int b = 0; b < NB; ++b)
@@ -324,7 +375,7 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
           for (int a = 0; a < NA; ++a)
 #pragma unroll
             for (int c = 0; c < NC; ++c) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoA + a) * n + g.aoC + c);
-          atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoD + d, s * double(acc));
+          if (active) atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoD + d, s * double(acc));
         }
     }
   }
@@ -339,71 +390,66 @@ struct RegMinBlocks {
   static constexpr int value = EST <= 120 ? 4 : (EST <= 150 ? 3 : 2);
 };
 
-constexpr int kBraPrimCache = 128;
+constexpr int kBraPrimCache = 64;
+constexpr int kRegWarps = 4;   // warps per block; each warp owns one work item
 
+// Register path, warp-granular: warp w of block b takes work item 4b+w,
+// caches its bra primitive pairs in a per-warp shared slot, processes its
+// kets 32 at a time, and reduces the bra-block J of density 0 with shuffles.
+// No block-wide barrier.
 template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
     jk_reg_kernel(JKArgs args) {
   using CI = ClassInfo<LA, LB, LC, LD>;
-  __shared__ double4 s_pp[kBraPrimCache];
-  __shared__ double2 s_aux[kBraPrimCache];
-  const int4 w = args.work[blockIdx.x];
-  int kb, ke;
-  ket_range(args, w, kb, ke);
+  using PA_t = typename PrimData<R>::A;
+  using PB_t = typename PrimData<R>::B;
+  __shared__ PA_t s_pp[kRegWarps][kBraPrimCache];
+  __shared__ PB_t s_aux[kRegWarps][kBraPrimCache];
+  __shared__ double s_jab[kRegWarps][CI::NAB];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.x * kRegWarps + warp;
+  if (item >= args.nwork) return;
+  const int4 w = args.work[item];
+  int kb = w.y, ke = w.z;
+  if (args.split_mode != 0) {
+    const int sp = args.split[item];
+    if (args.split_mode == 1) ke = min(ke, sp);
+    else kb = max(kb, sp);
+  }
   if (kb >= ke) return;
   const int bra = args.bra_pairs[w.x];
   const int4 pb = args.pair_info[bra];
   const bool cached = pb.w <= kBraPrimCache;
-  if (cached) {
-    for (int i = threadIdx.x; i < pb.w; i += blockDim.x) {
-      s_pp[i] = args.pp_data[pb.z + i];
-      s_aux[i] = args.pp_aux[pb.z + i];
+  if (cached)
+    for (int i = lane; i < pb.w; i += 32) {
+      s_pp[warp][i] = PrimData<R>::a(args, pb.z + i);
+      s_aux[warp][i] = PrimData<R>::b(args, pb.z + i);
     }
-  }
-  __syncthreads();
-  const double4* bpp = cached ? s_pp : args.pp_data + pb.z;
-  const double2* baux = cached ? s_aux : args.pp_aux + pb.z;
-  // J[a][b] of the fixed bra pair (single symmetric density): each loop
-  // iteration reduces the 32 lanes' contributions with shuffles into the
-  // warp's shared row; the rows are summed and added once per block.
-  __shared__ double s_jab[4][CI::NAB];
   const bool acc_j = args.with_j && args.nsym == 1;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (acc_j && lane < CI::NAB) s_jab[warp][lane] = 0.0;
-  if (acc_j && CI::NAB > 32)
-    for (int i = lane + 32; i < CI::NAB; i += 32) s_jab[warp][i] = 0.0;
+  for (int i = lane; i < CI::NAB; i += 32) s_jab[warp][i] = 0.0;
+  __syncwarp();
+  const PA_t* bpp = cached ? s_pp[warp] : (sizeof(R) == 4 ? (const PA_t*)(args.pp_f + pb.z)
+                                                         : (const PA_t*)(args.pp_data + pb.z));
+  const PB_t* baux = cached ? s_aux[warp] : (sizeof(R) == 4 ? (const PB_t*)(args.pp_f2 + pb.z)
+                                                           : (const PB_t*)(args.pp_aux + pb.z));
   QuartetGeom g;
-  for (int k0 = kb; k0 < ke; k0 += blockDim.x) {
-    const int k = k0 + threadIdx.x;
-    double jab[CI::NAB];
-#pragma unroll
-    for (int i = 0; i < CI::NAB; ++i) jab[i] = 0.0;
-    if (k < ke) {
-      load_quartet(args, bra, args.ket_pairs[k], g);
-      R out[CI::NOUT];
-      quartet_block_reg<LA, LB, LC, LD, R>(args, g, bpp, baux, out);
-      digest_reg<LA, LB, LC, LD, R>(args, g, out, acc_j, jab);
-    }
-    if (acc_j) {
-#pragma unroll
-      for (int ab = 0; ab < CI::NAB; ++ab) {
-        double v = jab[ab];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        if (lane == 0) s_jab[warp][ab] += v;
-      }
-    }
+  for (int k0 = kb; k0 < ke; k0 += 32) {
+    // lanes past the range recompute the last ket with their output masked,
+    // so the whole warp takes part in the J shuffles
+    const bool active = k0 + lane < ke;
+    const int k = active ? k0 + lane : ke - 1;
+    load_quartet(args, bra, args.ket_pairs[k], g);
+    R out[CI::NOUT];
+    quartet_block_reg<LA, LB, LC, LD, R>(args, g, bpp, baux, out);
+    digest_reg<LA, LB, LC, LD, R>(args, g, out, acc_j, active, s_jab[warp]);
   }
   if (acc_j) {
-    __syncthreads();
+    __syncwarp();
     const int4 ia = args.sh_info[pb.x], ib = args.sh_info[pb.y];
-    const long long base = args.mol_base[ia.z];
+    double* vj = args.vj + args.mol_base[ia.z];
     const int n = args.mol_n[ia.z];
-    double* vj = args.vj + base;
-    const int nw = (blockDim.x + 31) >> 5;
-    for (int ab = threadIdx.x; ab < CI::NAB; ab += blockDim.x) {
-      double v = 0.0;
-      for (int i = 0; i < nw; ++i) v += s_jab[i][ab];
+    for (int ab = lane; ab < CI::NAB; ab += 32) {
+      const double v = s_jab[warp][ab];
       if (v != 0.0) atomicAdd(vj + (long long)(ia.x + ab / CI::NB) * n + ib.x + ab % CI::NB, v);
     }
   }

@@ -89,7 +89,7 @@ struct Plan {
   // nuclei (for one-electron terms): global atm rows with charge
   std::vector<double4> atom_xyzq; // (x, y, z, charge) per global atm row
   // device tables
-  DevBuf d_ws_info, d_ws_xyz, d_pair_info, d_pp_data, d_pp_aux, d_pp_exp, d_mol_base_cart, d_mol_ncart,
+  DevBuf d_ws_info, d_ws_xyz, d_pair_info, d_pp_data, d_pp_aux, d_pp_exp, d_pp_f, d_pp_f2, d_mol_base_cart, d_mol_ncart,
       d_mol_base_out, d_mol_nout, d_cart_ws, d_out_ws, d_status, d_maxd, d_q_work, d_atoms,
       d_ws_atm, d_mol_ao_off, d_ws_prim, d_ws_prim_off;
   // one-electron work: every work pair of each pair class, nuclei ranges
