@@ -83,6 +83,9 @@ struct Tables {
   // (double) / 32-byte (float) row per lookup.
   const double* boys_m;
   const float* boys_m_f;
+  // FP32 copies at spacing 1/10 (401 rows of 8, terms F_{M+i}/i!), staged in
+  // shared memory by the FP32 register path.
+  const float* boys_s_f;
 };
 
 // Output-transform table layout: per l a kTW x kTW block, row = raw Cartesian
@@ -98,13 +101,13 @@ constexpr int kTS = kTW * kTW;
 //   F_{m+1} = ((2m+1) F_m - e^{-T}) / (2T).
 // (Taylor/downward scheme: Gill, Johnson & Pople, Int. J. Quantum Chem. 40, 745 (1991).)
 // Division-free: constant divisors are multiplications by folded reciprocals.
-template <int M, typename R>
-__device__ __forceinline__ void boys_fn(R t, R* f, const R* grid) {
-  static_assert(M == 1 || M == 3 || M == 5, "per-order tables exist for M = 1, 3, 5");
+template <int M, typename R, int SINV = 20, int NT = (sizeof(R) == 8 ? 8 : 5)>
+__device__ __forceinline__ void boys_fn(R t, R* f, const R* tab) {
+  // tab: this order's table, rows of 8 at spacing 1/SINV over [0, 40]
   if (t < R(40)) {
-    const int k = min(max(__float2int_rn(float(t) * 20.0f), 0), 800);
-    const R dt = R(k) * R(0.05) - t;          // -(t - t_k)
-    const R* row = grid + ((M - 1) / 2 * 801 + k) * 8;
+    const int k = min(max(__float2int_rn(float(t) * float(SINV)), 0), 40 * SINV);
+    const R dt = R(k) * R(1.0 / SINV) - t;          // -(t - t_k)
+    const R* row = tab + k * 8;
     R c[8];
     if constexpr (sizeof(R) == 8) {
       const double4 a = reinterpret_cast<const double4*>(row)[0];
@@ -115,8 +118,6 @@ __device__ __forceinline__ void boys_fn(R t, R* f, const R* grid) {
       const float4 b = reinterpret_cast<const float4*>(row)[1];
       c[0] = a.x; c[1] = a.y; c[2] = a.z; c[3] = a.w; c[4] = b.x; c[5] = b.y; c[6] = b.z; c[7] = b.w;
     }
-    // FP32 needs 5 terms (|dt| <= 0.025: truncation ~1e-10), FP64 all 8
-    constexpr int NT = sizeof(R) == 8 ? 8 : 5;
     R acc = c[NT - 1];
 #pragma unroll
     for (int i = NT - 2; i >= 0; --i) acc = c[i] + acc * dt;
@@ -147,16 +148,17 @@ template <> __device__ __forceinline__ float drcp<float>(float x) { return __frc
 // trigonometric formula in float and polishes each node with two Newton
 // steps in R.  Max relative error vs 60-digit values: 2e-15 (N <= 2),
 // 2e-14 (N = 3), both in FP64.
-template <int N, typename R>
-__device__ __forceinline__ void rys_small(R t, R* x, R* w, const R* grid) {
+template <int N, typename R, int SINV = 20, int NT = (sizeof(R) == 8 ? 8 : 5)>
+__device__ __forceinline__ void rys_small(R t, R* x, R* w, const R* tab) {
+  // tab: Taylor table of order M = 2N - 1
   if (N == 1) {
     R f[2];
-    boys_fn<1, R>(t, f, grid);
+    boys_fn<1, R, SINV, NT>(t, f, tab);
     w[0] = f[0];
     x[0] = f[1] * drcp<R>(f[0]);
   } else if (N == 2) {
     R f[4];
-    boys_fn<3, R>(t, f, grid);
+    boys_fn<3, R, SINV, NT>(t, f, tab);
     const R inv0 = drcp<R>(f[0]);
     const R a0 = f[1] * inv0;
     const R s11 = f[2] - a0 * f[1];
@@ -175,7 +177,7 @@ __device__ __forceinline__ void rys_small(R t, R* x, R* w, const R* grid) {
     w[1] = fb * drcp<R>(b1 + dp * dp);
   } else {
     R f[6];
-    boys_fn<5, R>(t, f, grid);
+    boys_fn<5, R, SINV, NT>(t, f, tab);
     const R inv0 = drcp<R>(f[0]);
     const R a0 = f[1] * inv0;
     const R s11 = f[2] - a0 * f[1], s12 = f[3] - a0 * f[2];
@@ -251,7 +253,7 @@ template <> struct TableSel<float> {
 template <int N, typename R>
 __device__ __forceinline__ void rys_roots(R t, R* x, R* w, const Tables& tb) {
   if (N <= 3) {
-    rys_small<N, R>(t, x, w, TableSel<R>::boys(tb));
+    rys_small<N, R>(t, x, w, TableSel<R>::boys(tb) + (N - 1) * 801 * 8);
     return;
   }
   const int nint = tb.rys_nint[N];
@@ -281,7 +283,7 @@ template <int N, typename R>
 __device__ __forceinline__ R rys_one(R t, int f, const Tables& tb) {
   if (N <= 3) {
     R x[N], w[N];
-    rys_small<N, R>(t, x, w, TableSel<R>::boys(tb));
+    rys_small<N, R>(t, x, w, TableSel<R>::boys(tb) + (N - 1) * 801 * 8);
     R v = x[0];
 #pragma unroll
     for (int i = 0; i < N; ++i) {

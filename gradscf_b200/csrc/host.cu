@@ -92,7 +92,7 @@ static void output_transform(int l, int cart, double* t /* [10][10] */) {
 // ---------------------------------------------------------------- tables
 struct DeviceTables {
   Tables t{};
-  DevBuf rys, rys_f, off, nint, ar, aw, boys, boys_f, c2s_sph, c2s_cart, boys_m, boys_m_f;
+  DevBuf rys, rys_f, off, nint, ar, aw, boys, boys_f, c2s_sph, c2s_cart, boys_m, boys_m_f, boys_s_f;
   Tables sph, cartt;
 };
 
@@ -130,6 +130,11 @@ static DeviceTables& tables_for(int device) {
         }
       }
     up(d->boys_m, bm.data(), bm.size() * sizeof(double));
+    std::vector<float> bs(3 * 401 * 8);
+    for (int mi = 0; mi < 3; ++mi)
+      for (int k = 0; k < 401; ++k)
+        for (int i = 0; i < 8; ++i) bs[(mi * 401 + k) * 8 + i] = float(bm[(mi * 801 + 2 * k) * 8 + i]);
+    up(d->boys_s_f, bs.data(), bs.size() * sizeof(float));
     std::vector<float> bmf(bm.begin(), bm.end());
     up(d->boys_m_f, bmf.data(), bmf.size() * sizeof(float));
   }
@@ -151,6 +156,7 @@ static DeviceTables& tables_for(int device) {
   base.boys_f = d->boys_f.as<float>();
   base.boys_m = d->boys_m.as<double>();
   base.boys_m_f = d->boys_m_f.as<float>();
+  base.boys_s_f = d->boys_s_f.as<float>();
   d->sph = base;
   d->sph.c2s = d->c2s_sph.as<double>();
   d->cartt = base;

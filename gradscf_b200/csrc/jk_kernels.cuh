@@ -239,7 +239,8 @@ __device__ __forceinline__ long long dm_index(const JKArgs& args, int mol, int a
 template <int LA, int LB, int LC, int LD, typename R>
 __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const QuartetGeom& g,
                                                   const typename PrimData<R>::A* bpp,
-                                                  const typename PrimData<R>::B* baux, R* out) {
+                                                  const typename PrimData<R>::B* baux, R* out,
+                                                  const float* s_boys) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   using GI = GIdx<LA, LB, LC, LD>;
   constexpr int N = CI::NROOT;
@@ -255,7 +256,10 @@ __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const Quar
       PrimQ<R> s;
       prim_any<R>(g, ac, bpp[i], baux[i], Q, QA, s);
       R x[N], w[N];
-      rys_roots<N, R>(s.t, x, w, args.tb);
+      if constexpr (sizeof(R) == 4 && N <= 3)
+        rys_small<N, float, 10, 6>(s.t, x, w, s_boys);   // shared-memory Taylor rows
+      else
+        rys_roots<N, R>(s.t, x, w, args.tb);
 #pragma unroll
       for (int r = 0; r < N; ++r) {
         RootCoef<R> rc;
@@ -386,8 +390,10 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
 template <int LA, int LB, int LC, int LD, typename R>
 struct RegMinBlocks {
   using CI = ClassInfo<LA, LB, LC, LD>;
-  static constexpr int EST = 2 * (CI::NOUT + 3 * CI::NG) + 56;   // same cap for FP32 and FP64
-  static constexpr int value = EST <= 120 ? 4 : (EST <= 150 ? 3 : 2);
+  // estimated live registers: output block + one root's 2D integrals + ~70 for
+  // addresses, primitive scalars and digestion (FP64 values take two)
+  static constexpr int EST = (sizeof(R) == 8 ? 2 : 1) * (CI::NOUT + 3 * CI::NG) + 70;
+  static constexpr int value = EST <= 84 ? 6 : (EST <= 100 ? 5 : (EST <= 124 ? 4 : (EST <= 160 ? 3 : 2)));
 };
 
 constexpr int kBraPrimCache = 64;
@@ -406,6 +412,15 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
   __shared__ PA_t s_pp[kRegWarps][kBraPrimCache];
   __shared__ PB_t s_aux[kRegWarps][kBraPrimCache];
   __shared__ double s_jab[kRegWarps][CI::NAB];
+  // FP32 path with closed-form roots: this order's Taylor table (12.8 KB)
+  constexpr bool kSharedBoys = sizeof(R) == 4 && CI::NROOT <= 3;
+  __shared__ __align__(16) float s_boys[kSharedBoys ? 401 * 8 : 4];
+  if constexpr (kSharedBoys) {
+    const float4* src = reinterpret_cast<const float4*>(args.tb.boys_s_f + (CI::NROOT - 1) * 401 * 8);
+    float4* dst = reinterpret_cast<float4*>(s_boys);
+    for (int i = threadIdx.x; i < 401 * 2; i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int item = blockIdx.x * kRegWarps + warp;
   if (item >= args.nwork) return;
@@ -440,7 +455,7 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
     const int k = active ? k0 + lane : ke - 1;
     load_quartet(args, bra, args.ket_pairs[k], g);
     R out[CI::NOUT];
-    quartet_block_reg<LA, LB, LC, LD, R>(args, g, bpp, baux, out);
+    quartet_block_reg<LA, LB, LC, LD, R>(args, g, bpp, baux, out, s_boys);
     digest_reg<LA, LB, LC, LD, R>(args, g, out, acc_j, active, s_jab[warp]);
   }
   if (acc_j) {
