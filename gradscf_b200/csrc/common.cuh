@@ -281,7 +281,10 @@ __device__ __forceinline__ void rys_roots(R t, R* x, R* w, const Tables& tb) {
 // several threads share one primitive quartet.
 template <int N, typename R>
 __device__ __forceinline__ R rys_one(R t, int f, const Tables& tb) {
-  if (N <= 3) {
+  // several lanes share the quartet: for N >= 3 each lane evaluates one
+  // Chebyshev series of the same interval (near-broadcast reads) instead of
+  // every lane running the closed-form solve
+  if (N <= 2) {
     R x[N], w[N];
     rys_small<N, R>(t, x, w, TableSel<R>::boys(tb) + (N - 1) * 801 * 8);
     R v = x[0];

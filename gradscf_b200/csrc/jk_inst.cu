@@ -22,6 +22,8 @@ template <int LA, int LB, int LC, int LD>
 struct Policy {
   using CI = ClassInfo<LA, LB, LC, LD>;
   static constexpr bool REG = (3 * CI::NG + CI::NOUT <= 96) && CI::NROOT <= 3;
+  // tile path: kets up to d x d (NCD <= 36), bra pair fits one block
+  static constexpr bool TILE = !REG && CI::NCD <= 36 && CI::NAB <= 128;
   static constexpr int TEAM = CI::NOUT <= 4 * 24 ? 4 : CI::NOUT <= 8 * 24 ? 8 : CI::NOUT <= 16 * 24 ? 16 : 32;
 };
 
@@ -31,6 +33,18 @@ int launch_class(const JKArgs& args, cudaStream_t stream) {
   using P = Policy<LA, LB, LC, LD>;
   if constexpr (P::REG) {
     jk_reg_kernel<LA, LB, LC, LD, R><<<(args.nwork + kRegWarps - 1) / kRegWarps, 32 * kRegWarps, 0, stream>>>(args);
+  } else if constexpr (P::TILE) {
+    using TC = TileCfg<LA, LB, LC, LD, R>;
+    constexpr size_t smem = TC::bytes();
+    if (smem > 48 * 1024) {
+      static bool configured = false;
+      if (!configured) {
+        cudaFuncSetAttribute(jk_tile_kernel<LA, LB, LC, LD, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        configured = true;
+      }
+    }
+    jk_tile_kernel<LA, LB, LC, LD, R><<<args.nwork, TC::THREADS, smem, stream>>>(args);
   } else {
     constexpr int TEAM = P::TEAM;
     using SM = TeamSmem<LA, LB, LC, LD, R, TEAM>;
@@ -113,7 +127,9 @@ void REG_NAME(BRA_CLASS, KET_CLASS)(DispatchTable& t) {
   t.jk32[id] = &launch_class<XA, XB, YA, YB, float>;
   t.grad64[id] = &launch_grad<XA, XB, YA, YB>;
   t.reg_path[id] = Policy<XA, XB, YA, YB>::REG;
-  t.team[id] = Policy<XA, XB, YA, YB>::REG ? 1 : Policy<XA, XB, YA, YB>::TEAM;
+  t.team[id] = Policy<XA, XB, YA, YB>::REG ? 1
+               : (Policy<XA, XB, YA, YB>::TILE ? TileCfg<XA, XB, YA, YB, double>::THREADS / 4
+                                               : Policy<XA, XB, YA, YB>::TEAM);
 #if BRA_CLASS == KET_CLASS
   t.schwarz[X] = &launch_schwarz<XA, XB>;
 #endif

@@ -668,6 +668,105 @@ __global__ void jk_team_kernel(JKArgs args) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Tile path for mid-size classes (ket shells up to d): a team of NAB lanes
+// per quartet, lane (a, b) owning one bra Cartesian pair and every ket pair
+// (c, d) of the block, so each root costs it 3 (LC+1)(LD+1) shared reads for
+// NC*ND outputs.  Kets of a work item share their primitive count and the
+// bra is fixed, so all teams of a block run the primitive loop in lockstep
+// (block barriers, no divergence).  Digestion stages the contracted block in
+// shared memory and spreads the target elements over the team.
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD, typename R>
+struct TileCfg {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  static constexpr int TEAM = CI::NAB;
+  static constexpr int Q = (128 / TEAM) > 0 ? (128 / TEAM) : 1;      // quartets per block
+  static constexpr int THREADS = Q * TEAM;
+  static constexpr int N = CI::NROOT;
+  static constexpr int NG = CI::NG;
+  static constexpr int KSTR = (LC + 1) * (LD + 1);                     // ket part of a G row
+  // per quartet slot: G (3N*NG R), roots (2N R), staged block (NOUT double)
+  static constexpr size_t G_BYTES = ((size_t)(3 * N * NG + 2 * N) * sizeof(R) + 15) / 16 * 16;
+  static constexpr size_t SLOT = G_BYTES + (size_t)CI::NOUT * 8;
+  static constexpr size_t bytes() { return SLOT * Q; }
+};
+
+template <int LA, int LB, int LC, int LD, typename R>
+__global__ void __launch_bounds__(128) jk_tile_kernel(JKArgs args) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using TC = TileCfg<LA, LB, LC, LD, R>;
+  using GI = GIdx<LA, LB, LC, LD>;
+  constexpr int N = TC::N, NG = TC::NG, TEAM = TC::TEAM;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int4 w = args.work[blockIdx.x];
+  int kb, ke;
+  ket_range(args, w, kb, ke);
+  if (kb >= ke) return;
+  const int team = threadIdx.x / TEAM, lane = threadIdx.x % TEAM;
+  R* G = reinterpret_cast<R*>(smem_raw + (size_t)team * TC::SLOT);
+  R* roots = G + 3 * N * NG;
+  double* V = reinterpret_cast<double*>(smem_raw + (size_t)team * TC::SLOT + TC::G_BYTES);
+  const int bra = args.bra_pairs[w.x];
+  // this lane's bra Cartesian pair
+  const int ia = lane / CI::NB, ib = lane % CI::NB;
+  const int bx = GI::idx(cart_lx(LA, ia), cart_lx(LB, ib), 0, 0);
+  const int by = GI::idx(cart_ly(LA, ia), cart_ly(LB, ib), 0, 0);
+  const int bz = GI::idx(cart_lz(LA, ia), cart_lz(LB, ib), 0, 0);
+  for (int k0 = kb; k0 < ke; k0 += TC::Q) {
+    const bool active = k0 + team < ke;
+    QuartetGeom g;
+    load_quartet(args, bra, args.ket_pairs[active ? k0 + team : ke - 1], g);
+    R acc[CI::NCD];
+#pragma unroll
+    for (int q = 0; q < CI::NCD; ++q) acc[q] = R(0);
+    for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
+      const double4 Qd = args.pp_data[j];
+      const double2 QA = args.pp_aux[j];
+      for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
+        PrimQ<R> s;
+        prim_setup<R>(g, args.pp_data[i], args.pp_aux[i], Qd, QA, s);
+        for (int f = lane; f < 2 * N; f += TEAM) roots[f] = rys_one<N, R>(s.t, f, args.tb);
+        __syncthreads();
+        for (int tsk = lane; tsk < 3 * N; tsk += TEAM) {
+          const int r = tsk / 3, ax = tsk - 3 * r;
+          RootCoef<R> rc;
+          root_coef<R>(s, roots[r], rc);
+          const R abd = ax == 0 ? R(g.abx) : (ax == 1 ? R(g.aby) : R(g.abz));
+          const R cdd = ax == 0 ? R(g.cdx) : (ax == 1 ? R(g.cdy) : R(g.cdz));
+          const R g00 = ax == 2 ? roots[N + r] * s.pref : R(1);
+          build_g<LA, LB, LC, LD, R>(rc.c00[ax], rc.c0p[ax], rc.b10, rc.b01, rc.b00, g00, abd, cdd,
+                                     G + (r * 3 + ax) * NG);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+          R vx[TC::KSTR], vy[TC::KSTR], vz[TC::KSTR];
+          const R* gx = G + (r * 3) * NG + bx;
+          const R* gy = G + (r * 3 + 1) * NG + by;
+          const R* gz = G + (r * 3 + 2) * NG + bz;
+#pragma unroll
+          for (int q = 0; q < TC::KSTR; ++q) { vx[q] = gx[q]; vy[q] = gy[q]; vz[q] = gz[q]; }
+          static_for<0, CI::NCD>([&](auto O) {
+            constexpr int cd = decltype(O)::value;
+            constexpr int ic = cd / CI::ND, id = cd % CI::ND;
+            constexpr int jx = cart_lx(LC, ic) * (LD + 1) + cart_lx(LD, id);
+            constexpr int jy = cart_ly(LC, ic) * (LD + 1) + cart_ly(LD, id);
+            constexpr int jz = cart_lz(LC, ic) * (LD + 1) + cart_lz(LD, id);
+            acc[cd] += vx[jx] * vy[jy] * vz[jz];
+          });
+        }
+        __syncthreads();
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < CI::NCD; ++q) V[lane * CI::NCD + q] = double(acc[q]);
+    __syncthreads();
+    if (active) team_digest<LA, LB, LC, LD, TEAM>(args, g, V, lane);
+    __syncthreads();
+  }
+}
+
 // Schwarz bound of one work pair: max over output-basis AO pairs (a,b) of
 // |(ab|ab)| (csrc/coulomb_shells.h:60-77 uses the same diagonal), one team
 // per pair.  c2s[l] holds the 10x7 output transform of shell l.
