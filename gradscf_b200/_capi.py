@@ -20,7 +20,7 @@ EXPORTS = (
     "b200jk_check_status", "b200jk_direct_jk_tables", "b200jk_direct_jk_geom_vjp",
     "b200jk_int1e", "b200jk_int1e_grad", "b200jk_plan_class_stats", "b200jk_plan_split_stats",
     "b200jk_plan_set_profiling", "b200jk_plan_profile", "b200jk_measure_fma_peak",
-    "b200jk_direct_jk_noalloc",
+    "b200jk_direct_jk_noalloc", "b200jk_graph_create", "b200jk_graph_launch", "b200jk_graph_destroy",
 )
 NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024
 NCLASS = 55
@@ -79,6 +79,10 @@ def lib():
     h.b200jk_plan_profile.argtypes = [vp, ctypes.POINTER(f64), ctypes.POINTER(f64), ctypes.POINTER(i32)]
     h.b200jk_measure_fma_peak.argtypes = [i32, ctypes.POINTER(f64), vp]
     h.b200jk_direct_jk_noalloc.argtypes = [vp, vp, i32, vp, i32, i32, i32, i32, f64, vp]
+    h.b200jk_graph_create.argtypes = [vp, vp, i32, vp, i32, i32, i32, i32, f64, ctypes.POINTER(vp)]
+    h.b200jk_graph_launch.argtypes = [vp, vp]
+    h.b200jk_graph_destroy.argtypes = [vp]
+    h.b200jk_graph_destroy.restype = None
     return h
 
 

@@ -949,6 +949,69 @@ int b200jk_direct_jk(b200jk_plan* plan, const double* d_density, int32_t nb, dou
   });
 }
 
+struct b200jk_graph {
+  b200jk_plan* plan;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+};
+
+int b200jk_graph_create(b200jk_plan* plan, const double* d_density, int32_t nb, double* d_out,
+                        int32_t with_j, int32_t with_k, int32_t hermi, int32_t precision,
+                        double fp32_cut, b200jk_graph** out) {
+  return guarded([&] {
+    if (!plan || !out) invalid("Null plan or output handle");
+    *out = nullptr;
+    Plan& p = *plan->p;
+    check_jk_args(p, d_density, nb, d_out, with_j, with_k, precision, fp32_cut);
+    CUDA_OK(cudaSetDevice(p.device));
+    ensure_scratch(p, nb);
+    cudaStream_t st;
+    CUDA_OK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    // one eager build first: first-use kernel attributes are set outside capture
+    run_jk_core(p, d_density, nb, d_out, with_j, with_k, hermi ? 1 : 0, precision, fp32_cut, st,
+                p.d_dens.as<double>(), p.d_dens_f.as<float>(), p.d_vj.as<double>(), p.d_vk.as<double>(),
+                false);
+    CUDA_OK(cudaStreamSynchronize(st));
+    cudaGraph_t graph = nullptr;
+    CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      run_jk_core(p, d_density, nb, d_out, with_j, with_k, hermi ? 1 : 0, precision, fp32_cut, st,
+                  p.d_dens.as<double>(), p.d_dens_f.as<float>(), p.d_vj.as<double>(),
+                  p.d_vk.as<double>(), false);
+    } catch (...) {
+      cudaStreamEndCapture(st, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      cudaStreamDestroy(st);
+      throw;
+    }
+    CUDA_OK(cudaStreamEndCapture(st, &graph));
+    cudaStreamDestroy(st);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      throw Failure{B200JK_INTERNAL, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+    }
+    *out = new b200jk_graph{plan, graph, exec};
+  });
+}
+
+int b200jk_graph_launch(b200jk_graph* g, void* stream) {
+  return guarded([&] {
+    if (!g) invalid("Null graph");
+    CUDA_OK(cudaSetDevice(g->plan->p->device));
+    CUDA_OK(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+  });
+}
+
+void b200jk_graph_destroy(b200jk_graph* g) {
+  if (!g) return;
+  cudaSetDevice(g->plan->p->device);
+  cudaGraphExecDestroy(g->exec);
+  cudaGraphDestroy(g->graph);
+  delete g;
+}
+
 int b200jk_check_status(b200jk_plan* plan, void* stream) {
   return guarded([&] {
     if (!plan) invalid("Null plan");

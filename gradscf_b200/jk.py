@@ -131,6 +131,46 @@ class DirectJKPlan:
         return j, k
 
 
+class JKGraph:
+    """A captured J/K build (``b200jk_graph_create``) on fixed buffers.
+
+    ``run(density)`` copies the (nb, packed_size) density into the graph's
+    input buffer and replays the captured build; the result lands in
+    ``self.out`` (nops, nb, packed_size).
+    """
+
+    def __init__(self, plan: DirectJKPlan, nb=1, *, with_j=True, with_k=True, hermi=1,
+                 precision="fp64", fp32_cut=DEFAULT_FP32_CUT):
+        self.plan = plan
+        nops = int(bool(with_j)) + int(bool(with_k))
+        self.inp = torch.zeros((nb, plan.packed_size), dtype=torch.float64, device=plan.device)
+        self.out = torch.zeros((nops, nb, plan.packed_size), dtype=torch.float64, device=plan.device)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(plan.device):
+            _capi.check(_capi.lib().b200jk_graph_create(
+                plan._h, ctypes.c_void_p(self.inp.data_ptr()), nb, ctypes.c_void_p(self.out.data_ptr()),
+                int(bool(with_j)), int(bool(with_k)), int(bool(hermi)), PRECISIONS[precision],
+                float(fp32_cut), ctypes.byref(h)))
+        self._h = h
+
+    def run(self, density, stream=None):
+        self.inp.copy_(density.reshape(self.inp.shape))
+        with torch.cuda.device(self.plan.device):
+            _capi.check(_capi.lib().b200jk_graph_launch(self._h, _stream_handle(stream)))
+        return self.out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _capi.lib().b200jk_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 _PLAN_CACHE: "OrderedDict[tuple, DirectJKPlan]" = OrderedDict()
 
 

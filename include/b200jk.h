@@ -121,6 +121,20 @@ int b200jk_direct_jk_noalloc(b200jk_plan* plan, const double* d_density, int32_t
                              int32_t with_j, int32_t with_k, int32_t hermi, int32_t precision,
                              double fp32_cut, void* stream);
 
+/* CUDA-graph capture of one complete J/K build (density transform, every
+ * class-pair kernel, finalisation) for fixed device buffers, replayed once
+ * per SCF iteration: the reference runs one FFI call per iteration
+ * (scf/rks.py:305-321); here the caller copies the next density into
+ * d_density and launches the graph.  Creation runs one eager build (which
+ * allocates the plan's scratch) before capturing.  The graph uses the plan's
+ * scratch: do not run another build on the same plan concurrently. */
+typedef struct b200jk_graph b200jk_graph;
+int b200jk_graph_create(b200jk_plan* plan, const double* d_density, int32_t nb, double* d_out,
+                        int32_t with_j, int32_t with_k, int32_t hermi, int32_t precision,
+                        double fp32_cut, b200jk_graph** out);
+int b200jk_graph_launch(b200jk_graph* graph, void* stream);
+void b200jk_graph_destroy(b200jk_graph* graph);
+
 /* Synchronise `stream` and turn the plan's device status word into a return
  * code (nonfinite density -> B200JK_INVALID_ARGUMENT), clearing it. */
 int b200jk_check_status(b200jk_plan* plan, void* stream);
