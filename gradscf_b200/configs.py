@@ -1,0 +1,168 @@
+"""Run the workload configurations of the J/K build and print one JSON record each.
+
+    python -m gradscf_b200.configs c0|c2|c3|c4 [--quick]
+
+c0  water cc-pVDZ (24 functions): FP64 RHF (Schwarz 1e-12, conv_tol 1e-10) and
+    one J/K build of D = C C^T, C ~ N(0,1)/sqrt(24), 5 columns, seed 0.
+c2  (H2O)16 6-31G* (seed 2): RHF forces in FP64 and split mode; central
+    differences (step 1e-4 Bohr) on 6 random coordinates (seed 2).
+c3  256 water clusters, N ~ U{1..24} (seed 3), cluster m from seed 1000+m,
+    cc-pVDZ: one batched plan, one packed (graph-replayed) J/K build per SCF
+    iteration for all clusters; aggregate quartets/s, FP64 vs split, and the
+    per-cluster energy difference.
+c4  (H2O)64 cc-pVTZ (3712 functions, seed 4): J/K builds in FP64 and split
+    mode along an RHF SCF (fragment guess, 15 iterations) and one force.
+Geometry generator and seeds: gradscf_b200/workloads.py.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+import torch
+
+from . import scf as S
+from . import workloads as W
+
+
+def _events():
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _fragments(spec, n):
+    atoms = spec.split("; ")
+    return ["; ".join(atoms[3 * i:3 * i + 3]) for i in range(n)]
+
+
+def run_c0():
+    mol = S.Molecule(W.WATER, "cc-pvdz", cart=False, schwarz_cut=1e-12)
+    res = S.rhf(mol, conv_tol=1e-10)
+    d = torch.as_tensor(W.psd_density(mol.nao, 5, 0), device=mol.device)
+    for _ in range(3):
+        mol.jk(d)
+    e0, e1 = _events()
+    e0.record()
+    j, k = mol.jk(d)
+    e1.record()
+    torch.cuda.synchronize()
+    return {"config": "c0", "nao": mol.nao, "rhf_energy_hartree": res.energy, "converged": res.converged,
+            "cycles": res.cycles, "jk_ms_psd_density": e0.elapsed_time(e1), "quartets": mol.plan.quartets}
+
+
+def run_c2(nwater=16, seed=2, npick=6):
+    spec = W.water_cluster(nwater, seed)
+    out = {"config": "c2", "system": f"(H2O){nwater} 6-31G* seed {seed}"}
+    grads = {}
+    syms = ["O", "H", "H"] * nwater
+    for precision in ("fp64", "split"):
+        mol = S.Molecule(spec, "6-31g*", cart=False, schwarz_cut=1e-12)
+        d0 = S.fragment_guess(mol, _fragments(spec, nwater), "6-31g*")
+        t0 = time.perf_counter()
+        res = S.rhf(mol, conv_tol=1e-12, conv_tol_grad=1e-9, precision=precision, density0=d0)
+        e0, e1 = _events()
+        e0.record()
+        g = S.rhf_gradient(mol, res)
+        e1.record()
+        torch.cuda.synchronize()
+        grads[precision] = g
+        out[precision] = {"energy_hartree": res.energy, "cycles": res.cycles,
+                          "gradient_ms": e0.elapsed_time(e1), "scf_s": time.perf_counter() - t0}
+        rng = np.random.default_rng(seed)
+        picks = [(int(rng.integers(len(mol.charges))), int(rng.integers(3))) for _ in range(npick)]
+        h = 1e-4
+        diffs = []
+        for a, x in picks:
+            vals = []
+            for sgn in (1, -1):
+                c = mol.coords.copy()
+                c[a, x] += sgn * h
+                m = S.Molecule([(s_, tuple(v)) for s_, v in zip(syms, c)], "6-31g*", unit="Bohr",
+                               cart=False, schwarz_cut=1e-12)
+                vals.append(S.rhf(m, conv_tol=1e-12, conv_tol_grad=1e-9, precision=precision,
+                                  density0=res.density).energy)
+            fd = (vals[0] - vals[1]) / (2 * h)
+            diffs.append(abs(fd - g[a, x]))
+        out[precision]["max_abs_fd_minus_analytic"] = float(max(diffs))
+        out[precision]["net_force"] = float(np.abs(g.sum(0)).max())
+    out["max_abs_force_split_minus_fp64"] = float(np.abs(grads["split"] - grads["fp64"]).max())
+    return out
+
+
+def run_c3(count=256, quick=False):
+    sizes = W.batch_sizes(count=count, seed=3)
+    if quick:
+        sizes = sizes[:16]
+    specs = [W.water_cluster(int(nw), 1000 + m) for m, nw in enumerate(sizes)]
+    batch = S.MoleculeBatch(specs, "cc-pvdz", cart=False, schwarz_cut=1e-12)
+    # fragment guess: every monomer of every cluster in one batched SCF
+    monomers = [f for spec, nw in zip(specs, sizes) for f in _fragments(spec, int(nw))]
+    mono = S.MoleculeBatch(monomers, "cc-pvdz", cart=False, schwarz_cut=1e-12)
+    _, mds, _, _, _ = S.rhf_batch(mono, conv_tol=1e-9, timing=False)
+    d0, pos = [], 0
+    for nw in sizes:
+        blocks = mds[pos:pos + int(nw)]
+        pos += int(nw)
+        d0.append(torch.block_diag(*blocks))
+    out = {"config": "c3", "molecules": len(specs), "nao_min": int(min(batch.nao)),
+           "nao_max": int(max(batch.nao)), "quartets_per_build": batch.plan.quartets}
+    energies = {}
+    for precision in ("fp64", "split"):
+        en, _, ms, cycles, conv = S.rhf_batch(batch, conv_tol=1e-10, precision=precision, use_graph=True,
+                                              density0=d0)
+        energies[precision] = en
+        steady = ms[1:] if len(ms) > 1 else ms
+        out[precision] = {"cycles": cycles, "converged": int(conv.sum()),
+                          "ms_per_build": float(np.mean(steady)),
+                          "quartets_per_s": batch.plan.quartets / (np.mean(steady) * 1e-3)}
+    out["split_speedup"] = out["fp64"]["ms_per_build"] / out["split"]["ms_per_build"]
+    out["max_abs_dE_per_molecule_hartree"] = float(np.abs(energies["split"] - energies["fp64"]).max())
+    return out
+
+
+def run_c4(nwater=64, seed=4, cycles=15, quick=False):
+    if quick:
+        nwater = 8
+    spec = W.water_cluster(nwater, seed)
+    t0 = time.perf_counter()
+    mol = S.Molecule(spec, "cc-pvtz", cart=False, schwarz_cut=1e-12)
+    plan_s = time.perf_counter() - t0
+    d0 = S.fragment_guess(mol, _fragments(spec, nwater), "cc-pvtz")
+    out = {"config": "c4", "nao": mol.nao, "quartets_per_build": mol.plan.quartets, "plan_s": plan_s}
+    energies = {}
+    for precision in ("fp64", "split"):
+        res = S.rhf(mol, precision=precision, density0=d0, fixed_cycles=cycles, use_graph=True)
+        energies[precision] = res.energy
+        ms = res.jk_ms[1:]
+        out[precision] = {"s_per_iter": float(np.mean(ms)) * 1e-3,
+                          "quartets_per_s": mol.plan.quartets / (np.mean(ms) * 1e-3),
+                          "energy_hartree": res.energy,
+                          "last_iter_dE": abs(res.energies[-1] - res.energies[-2])}
+        if precision == "split":
+            e0, e1 = _events()
+            e0.record()
+            g = S.rhf_gradient(mol, res)
+            e1.record()
+            torch.cuda.synchronize()
+            out["force_ms"] = e0.elapsed_time(e1)
+            out["net_force"] = float(np.abs(g.sum(0)).max())
+    out["split_speedup"] = out["fp64"]["s_per_iter"] / out["split"]["s_per_iter"]
+    out["abs_dE_hartree"] = abs(energies["split"] - energies["fp64"])
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("config", choices=("c0", "c2", "c3", "c4"))
+    ap.add_argument("--quick", action="store_true", help="reduced size (smoke run)")
+    a = ap.parse_args(argv)
+    fn = {"c0": run_c0, "c2": run_c2, "c3": lambda: run_c3(quick=a.quick),
+          "c4": lambda: run_c4(quick=a.quick)}[a.config]
+    if a.config == "c2" and a.quick:
+        fn = lambda: run_c2(nwater=4)  # noqa: E731
+    print(json.dumps(fn()))
+
+
+if __name__ == "__main__":
+    main()

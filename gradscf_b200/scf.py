@@ -234,79 +234,115 @@ class MoleculeBatch:
 
 
 def rhf_batch(batch: MoleculeBatch, *, conv_tol=1e-10, max_cycle=60, precision="fp64",
-              fp32_cut=DEFAULT_FP32_CUT, diis_space=8, timing=True):
-    """RHF of every molecule of the batch; one packed J/K build per iteration
-    serves all molecules.  Returns (energies, densities, jk_ms, cycles, converged)."""
+              fp32_cut=DEFAULT_FP32_CUT, diis_space=8, timing=True, use_graph=False,
+              fixed_cycles=None, density0=None):
+    """RHF of every molecule of the batch, vectorised over molecules of equal
+    (nao, nocc): batched Fock/energy/DIIS/eigh in torch, and ONE packed J/K
+    build (optionally a replayed CUDA graph) per iteration for all molecules.
+
+    Returns (energies ndarray, densities list, jk_ms list, cycles, converged ndarray).
+    """
     dev = batch.device
+    plan = batch.plan
     s_all, h_all = batch.int1e("ovlp"), batch.int1e("kin") + batch.int1e("nuc")
     nm = len(batch.mols)
-    xs, ds, hs, ss = [], [], [], []
+    keys = {}
     for m in range(nm):
-        s = batch.block(s_all, m)
-        h = batch.block(h_all, m)
-        w, v = torch.linalg.eigh(s)
-        x = v / torch.sqrt(w)
-        e, c = _solve(h, x)
-        nocc = batch.mols[m]["nelectron"] // 2
-        xs.append(x); hs.append(h); ss.append(s)
-        ds.append(2.0 * c[:, :nocc] @ c[:, :nocc].T)
-    d_last = torch.zeros((batch.plan.packed_size,), dtype=torch.float64, device=dev)
-    jk = torch.zeros((2, batch.plan.packed_size), dtype=torch.float64, device=dev)
-    hist = [([], []) for _ in range(nm)]
-    e_old = [None] * nm
-    done = [False] * nm
-    energies = [0.0] * nm
+        keys.setdefault((batch.nao[m], batch.mols[m]["nelectron"] // 2), []).append(m)
+    groups = []
+    for (n, nocc), ms in keys.items():
+        base = torch.as_tensor([batch.offsets[m] for m in ms], device=dev, dtype=torch.int64)
+        idx = base[:, None] + torch.arange(n * n, device=dev)[None, :]
+        S = s_all[idx].view(-1, n, n)
+        H = h_all[idx].view(-1, n, n)
+        w, v = torch.linalg.eigh(S)
+        X = v / torch.sqrt(w)[:, None, :]
+        if density0 is None:
+            e, c = torch.linalg.eigh(X.transpose(1, 2) @ H @ X)
+            C = X @ c
+            D = 2.0 * C[:, :, :nocc] @ C[:, :, :nocc].transpose(1, 2)
+        else:
+            D = torch.stack([density0[m] for m in ms]).to(dev)
+        enuc = torch.as_tensor([batch.mols[m]["e_nuc"] for m in ms], device=dev, dtype=torch.float64)
+        groups.append(dict(ms=ms, n=n, nocc=nocc, idx=idx, S=S, H=H, X=X, D=D, enuc=enuc, hf=[], he=[],
+                           e_old=None, done=torch.zeros(len(ms), dtype=torch.bool, device=dev),
+                           energy=torch.zeros(len(ms), dtype=torch.float64, device=dev)))
+    packed = plan.packed_size
+    d_last = torch.zeros(packed, dtype=torch.float64, device=dev)
+    jk = torch.zeros((2, packed), dtype=torch.float64, device=dev)
+    graph = None
+    if use_graph:
+        from .jk import JKGraph
+        graph = JKGraph(plan, 1, hermi=1, precision=precision, fp32_cut=fp32_cut)
     jk_ms = []
     stream = torch.cuda.current_stream(dev)
-    conv_tol_grad = float(np.sqrt(conv_tol))
+    tol_grad = float(np.sqrt(conv_tol))
+    ncyc = fixed_cycles if fixed_cycles is not None else max_cycle
     cycle = 0
-    for cycle in range(1, max_cycle + 1):
-        d_packed = torch.cat([d.reshape(-1) for d in ds])
-        delta = (d_packed - d_last).reshape(1, -1).contiguous()
+    for cycle in range(1, ncyc + 1):
+        d_packed = torch.zeros(packed, dtype=torch.float64, device=dev)
+        for g in groups:
+            d_packed[g["idx"].reshape(-1)] = g["D"].reshape(-1)
+        delta = (d_packed - d_last).reshape(1, -1)
         if timing:
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ev0.record(stream)
-        out = batch.plan.jk_packed(delta, hermi=1, precision=precision, fp32_cut=fp32_cut)
+        out = graph.run(delta) if graph is not None else plan.jk_packed(
+            delta.contiguous(), hermi=1, precision=precision, fp32_cut=fp32_cut, check=False)
         if timing:
             ev1.record(stream)
             jk_ms.append((ev0, ev1))
         jk += out[:, 0]
         d_last = d_packed
-        for m in range(nm):
-            if done[m]:
-                continue
-            d, h, s, x = ds[m], hs[m], ss[m], xs[m]
-            j, k = batch.block(jk[0], m), batch.block(jk[1], m)
-            f = h + j - 0.5 * k
-            en = (torch.sum(d * h) + 0.5 * torch.sum(d * j) - 0.25 * torch.sum(d * k)).item() + batch.mols[m]["e_nuc"]
-            energies[m] = en
-            err_o = x.T @ (f @ d @ s - s @ d @ f) @ x
-            if e_old[m] is not None and abs(en - e_old[m]) < conv_tol and torch.linalg.norm(err_o).item() < conv_tol_grad:
-                done[m] = True
-                continue
-            hf, he = hist[m]
-            hf.append(f); he.append(err_o)
-            del hf[:-diis_space], he[:-diis_space]
-            if len(hf) > 1:
-                k_ = len(hf)
-                b = -torch.ones((k_ + 1, k_ + 1), dtype=torch.float64, device=dev)
-                b[k_, k_] = 0.0
-                for a in range(k_):
-                    for c_ in range(a, k_):
-                        b[a, c_] = b[c_, a] = torch.sum(he[a] * he[c_])
-                rhs = torch.zeros(k_ + 1, dtype=torch.float64, device=dev)
-                rhs[k_] = -1.0
-                coef = torch.linalg.solve(b, rhs)[:k_]
-                f = sum(cf * fi for cf, fi in zip(coef, hf))
-            e, c = _solve(f, x)
-            nocc = batch.mols[m]["nelectron"] // 2
-            ds[m] = 2.0 * c[:, :nocc] @ c[:, :nocc].T
-            e_old[m] = en
-        if all(done):
+        all_done = True
+        for g in groups:
+            n = g["n"]
+            J = jk[0][g["idx"]].view(-1, n, n)
+            K = jk[1][g["idx"]].view(-1, n, n)
+            D, H, S, X = g["D"], g["H"], g["S"], g["X"]
+            F = H + J - 0.5 * K
+            en = (D * H).sum((1, 2)) + 0.5 * (D * J).sum((1, 2)) - 0.25 * (D * K).sum((1, 2)) + g["enuc"]
+            err = X.transpose(1, 2) @ (F @ D @ S - S @ D @ F) @ X
+            gn = torch.linalg.norm(err, dim=(1, 2))
+            if g["e_old"] is not None:
+                g["done"] = g["done"] | (((en - g["e_old"]).abs() < conv_tol) & (gn < tol_grad))
+            g["energy"] = en
+            g["e_old"] = en
+            if not bool(g["done"].all()):
+                all_done = False
+            g["hf"].append(F)
+            g["he"].append(err)
+            del g["hf"][:-diis_space], g["he"][:-diis_space]
+            k_ = len(g["hf"])
+            if k_ > 1:
+                E = torch.stack(g["he"], 1)                       # (G, k, n, n)
+                Bm = -torch.ones((E.shape[0], k_ + 1, k_ + 1), dtype=torch.float64, device=dev)
+                Bm[:, :k_, :k_] = torch.einsum("gaij,gbij->gab", E, E)
+                Bm[:, k_, k_] = 0.0
+                rhs = torch.zeros((E.shape[0], k_ + 1), dtype=torch.float64, device=dev)
+                rhs[:, k_] = -1.0
+                coef = torch.linalg.solve(Bm, rhs)[:, :k_]
+                F = torch.einsum("gk,gkij->gij", coef, torch.stack(g["hf"], 1))
+            e, c = torch.linalg.eigh(X.transpose(1, 2) @ F @ X)
+            C = X @ c
+            g["D"] = 2.0 * C[:, :, :g["nocc"]] @ C[:, :, :g["nocc"]].transpose(1, 2)
+        if all_done and fixed_cycles is None:
             break
     torch.cuda.synchronize(dev)
+    if graph is not None:
+        graph.close()
+    energies = np.zeros(nm)
+    converged = np.zeros(nm, dtype=bool)
+    densities = [None] * nm
+    for g in groups:
+        en = g["energy"].cpu().numpy()
+        dn = g["done"].cpu().numpy()
+        for i, m in enumerate(g["ms"]):
+            energies[m] = en[i]
+            converged[m] = dn[i]
+            densities[m] = g["D"][i]
     times = [a.elapsed_time(b) for a, b in jk_ms] if timing else []
-    return energies, ds, times, cycle, done
+    return energies, densities, times, cycle, converged
 
 
 def fragment_guess(mol: Molecule, fragments, basis, *, unit="Angstrom"):

@@ -77,3 +77,18 @@ def test_water_cc_pvdz_rhf_fp64_vs_oracle_and_split():
     assert res.converged and abs(res.energy - ref["energy"]) < 1e-9
     split = S.rhf(mol, conv_tol=1e-10, precision="split")
     assert split.converged and abs(split.energy - res.energy) < 1e-8
+
+
+@pytest.mark.parametrize("precision,use_graph", [("fp64", False), ("split", True)])
+def test_batched_rhf_matches_single_molecule_rhf(precision, use_graph):
+    # uneven batch: two clusters of equal size share a vectorised group
+    from gradscf_b200 import workloads as W
+    specs = [W.water_cluster(n, 1000 + i) for i, n in enumerate((1, 3, 2, 3))]
+    batch = S.MoleculeBatch(specs, "cc-pvdz", cart=False, schwarz_cut=1e-12)
+    en, ds, ms, cycles, conv = S.rhf_batch(batch, conv_tol=1e-10, precision=precision, use_graph=use_graph)
+    assert conv.all() and len(ms) == cycles
+    for m, spec in enumerate(specs):
+        mol = S.Molecule(spec, "cc-pvdz", cart=False, schwarz_cut=1e-12)
+        ref = S.rhf(mol, conv_tol=1e-10, precision=precision)
+        assert abs(en[m] - ref.energy) < 1e-8, (m, en[m], ref.energy)
+        assert ds[m].shape == (mol.nao, mol.nao)
