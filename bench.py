@@ -141,6 +141,10 @@ def main():
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--nwater", type=int, default=32,
                     help="cluster size (profiling runs use a smaller case; the benchmark is 32)")
+    ap.add_argument("--eager", action="store_true",
+                    help="launch the J/K kernels one by one instead of replaying a captured CUDA graph")
+    ap.add_argument("--class-times", action="store_true",
+                    help="add every class pair's per-step kernel time (both modes) to the line")
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline leg (profiling runs)")
     args = ap.parse_args()
@@ -155,7 +159,7 @@ def main():
         value, cores, sample, step_s = cpu_reference_run(args.steps, args.warmup)
         line = {"metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "impl": "reference",
                 "config": {"workload": WORKLOAD, "sample": sample},
                 "cpu_baseline": {"value": value, "unit": "quartets/s", "cores": cores,
@@ -167,6 +171,7 @@ def main():
 
     import torch
     from gradscf_b200 import _capi, flop_model, scf, workloads
+    from gradscf_b200.jk import JKGraph
     import ctypes
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -188,6 +193,10 @@ def main():
     frags = ["; ".join(atoms[3 * i:3 * i + 3]) for i in range(args.nwater)]
     d0 = scf.fragment_guess(mol, frags, "cc-pvdz")
     plan = mol.plan
+    if world > 1:
+        # one J/K build shared by the ranks: cost-balanced work-item shards,
+        # partial J/K summed by an NCCL all-reduce inside every build
+        plan.set_shard(rank, world)
     n = mol.nao
     quartets = plan.quartets
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -206,7 +215,8 @@ def main():
     W, K = args.warmup, args.steps
     total = W + K
 
-    results, deltas_split = {}, []
+    results, deltas = {}, {"fp64": [], "split": []}
+    deltas_split = deltas["split"]
     clocks = ClockSampler(local)
     with clocks:
         for precision in ("fp64", "split"):
@@ -227,23 +237,30 @@ def main():
                         if dist:
                             dist.barrier()
                         torch.cuda.synchronize()
-                        lib.b200jk_plan_set_profiling(plan._h, 1)
                     acc["maxdd"].append(delta.abs().max().item())
-                    if precision == "split":
-                        deltas_split.append(delta.detach().to("cpu").pin_memory())
+                    deltas[precision].append(delta.detach().to("cpu").pin_memory())
                     flush.zero_()
 
             res = scf.rhf(mol, precision=precision, fp32_cut=FP32_CUT, fixed_cycles=total, on_jk=on_jk,
-                          density0=d0)
+                          density0=d0, use_graph=not args.eager)
             torch.cuda.synchronize()
             if precision == "split":
                 read_split_stats()
             if dist:
                 dist.barrier()
+            step_ms = float(np.mean(res.jk_ms[W:]))
+            # per-class kernel times: the same K builds replayed with
+            # per-launch events (kept out of the timed builds above)
+            lib.b200jk_plan_set_profiling(plan._h, 1)
+            dprof = torch.empty((1, n * n), dtype=torch.float64, device=dev)
+            for delta in deltas[precision]:
+                dprof.copy_(delta.reshape(1, n * n))
+                flush.zero_()
+                plan.jk_packed(dprof, hermi=1, precision=precision, fp32_cut=FP32_CUT, check=False)
+            torch.cuda.synchronize()
             lib.b200jk_plan_set_profiling(plan._h, 0)
             ms64 = (ctypes.c_double * nc)(); ms32 = (ctypes.c_double * nc)(); nl = (ctypes.c_int32 * nc)()
             _capi.check(lib.b200jk_plan_profile(plan._h, ms64, ms32, nl))
-            step_ms = float(np.mean(res.jk_ms[W:]))
             if dist:
                 t = torch.tensor([step_ms], device=dev)
                 dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -259,25 +276,33 @@ def main():
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
+        graph = None if args.eager else JKGraph(plan, 1, hermi=1, precision="split", fp32_cut=FP32_CUT)
         for delta in deltas_split:
             hd.copy_(delta.reshape(1, n * n))
             flush.zero_()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            dd.copy_(hd, non_blocking=True)
-            plan.jk_packed(dd, hermi=1, precision="split", fp32_cut=FP32_CUT, out=out, check=False)
-            hout.copy_(out, non_blocking=True)
+            if graph is not None:
+                graph.inp.copy_(hd, non_blocking=True)
+                res_out = graph.launch()
+            else:
+                dd.copy_(hd, non_blocking=True)
+                res_out = plan.jk_packed(dd, hermi=1, precision="split", fp32_cut=FP32_CUT, out=out, check=False)
+            hout.copy_(res_out, non_blocking=True)
             e1.record(stream)
             e2e.append((e0, e1))
+            stream.synchronize()   # the host reads this step's result before reusing hd / hout
         torch.cuda.synchronize()
+        if graph is not None:
+            graph.close()
         e2e_step = float(np.mean([a.elapsed_time(b) for a, b in e2e]))
         if dist:
             t = torch.tensor([e2e_step], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_step = t.item()
 
-    qps = {p_: world * quartets / (results[p_]["ms"] * 1e-3) for p_ in results}
+    qps = {p_: quartets / (results[p_]["ms"] * 1e-3) for p_ in results}
     r64, r32 = results["fp64"]["res"], results["split"]["res"]
     acc = results["split"]["acc"]
 
@@ -310,14 +335,15 @@ def main():
     gpu_launches = K * (2 + 1 + 1 + nclasspairs + 2 * nclasspairs)
     line = {"metric": METRIC, "value": qps["split"], "unit": "quartets/s", "n_gpus": world,
             "steps": K, "warmup": W, "ms_per_step": results["split"]["ms"],
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f32/f64 split (f64 accumulation)", "data": "synthetic",
             "config": {"workload": WORKLOAD if args.nwater == 32 else f"(H2O){args.nwater} cc-pVDZ (profiling case)",
                        "step": "one RHF iteration's incremental J/K build (dD = D - D_last)",
+                       "launch": "eager kernel launches" if args.eager else "one CUDA-graph replay per build",
                        "scf": f"fragment guess (converged monomer densities), DIIS(8), {W} untimed + {K} timed iterations per mode",
                        "quartets_per_build": quartets, "nao": n, "fp32_cut": FP32_CUT,
                        "l2": "flushed (512 MB write) before every timed build",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"J/K work-item shards x{world} + NCCL all-reduce" if world > 1 else "single GPU"},
             "s_per_iter": {"split": results["split"]["ms"] * 1e-3, "fp64": results["fp64"]["ms"] * 1e-3},
             "fp64": fp64_build,
             "split_speedup_vs_fp64": results["fp64"]["ms"] / results["split"]["ms"],
@@ -326,11 +352,21 @@ def main():
                        "last_iter_dE_fp64": abs(r64.energies[-1] - r64.energies[-2])},
             "split_fraction_fp32_quartets": float(acc["q32"].sum() / max(1.0, acc["q32"].sum() + acc["q64"].sum())),
             "max_abs_dD_timed": [float(x) for x in acc["maxdd"]],
-            "e2e": {"value": world * quartets / (e2e_step * 1e-3), "unit": "quartets/s",
+            "e2e": {"value": quartets / (e2e_step * 1e-3), "unit": "quartets/s",
                     "ms_per_step": e2e_step, "h2d_bytes_per_step": int(n * n * 8),
                     "d2h_bytes_per_step": int(2 * n * n * 8)},
             "roofline": roofline, "gpu_launches": gpu_launches, "clocks": clocks.summary(),
             "top_kernels_split_step": top[:8]}
+    if args.class_times:
+        def _ct(mode):
+            out = {}
+            for c_ in range(nc):
+                for kind_, arr in (("f64", results[mode]["ms64"]), ("f32", results[mode]["ms32"])):
+                    if arr[c_] > 0:
+                        name = "({}{}|{}{})".format(*classes[c_])
+                        out[f"{name}{kind_}"] = round(arr[c_] / K, 4)
+            return out
+        line["class_ms_per_step"] = {"split": _ct("split"), "fp64": _ct("fp64")}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         value, cores, sample, _ = cpu_reference_run(1, 0)
         line["cpu_baseline"] = {"value": value, "unit": "quartets/s", "cores": cores,

@@ -21,6 +21,7 @@ EXPORTS = (
     "b200jk_int1e", "b200jk_int1e_grad", "b200jk_plan_class_stats", "b200jk_plan_split_stats",
     "b200jk_plan_set_profiling", "b200jk_plan_profile", "b200jk_measure_fma_peak",
     "b200jk_direct_jk_noalloc", "b200jk_graph_create", "b200jk_graph_launch", "b200jk_graph_destroy",
+    "b200jk_partition_items", "b200jk_plan_set_shard",
 )
 NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024
 NCLASS = 55
@@ -76,6 +77,8 @@ def lib():
     h.b200jk_plan_class_stats.argtypes = [vp, p64, p64]
     h.b200jk_plan_split_stats.argtypes = [vp, vp, p64, p64, p64, p64]
     h.b200jk_plan_set_profiling.argtypes = [vp, i32]
+    h.b200jk_partition_items.argtypes = [vp, i64, i32, vp]
+    h.b200jk_plan_set_shard.argtypes = [vp, i32, i32]
     h.b200jk_plan_profile.argtypes = [vp, ctypes.POINTER(f64), ctypes.POINTER(f64), ctypes.POINTER(i32)]
     h.b200jk_measure_fma_peak.argtypes = [i32, ctypes.POINTER(f64), vp]
     h.b200jk_direct_jk_noalloc.argtypes = [vp, vp, i32, vp, i32, i32, i32, i32, f64, vp]
@@ -95,3 +98,14 @@ def check(rc):
     if rc == UNSUPPORTED:
         raise Unsupported(rc, msg)
     raise B200JKError(rc, msg)
+
+
+def partition_items(cost, world):
+    """Owner rank of each work item: contiguous, cost-balanced blocks
+    (b200jk_partition_items; host-only, no GPU needed)."""
+    import numpy as np
+    c = np.ascontiguousarray(cost, dtype=np.int64)
+    owner = np.empty(c.shape[0], dtype=np.int32)
+    check(lib().b200jk_partition_items(c.ctypes.data_as(ctypes.c_void_p), c.shape[0], int(world),
+                                       owner.ctypes.data_as(ctypes.c_void_p)))
+    return owner

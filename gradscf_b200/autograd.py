@@ -89,6 +89,7 @@ class _DirectJK(torch.autograd.Function):
                 _capi.check(_capi.lib().b200jk_direct_jk_geom_vjp(
                     plan._h, ctypes.c_void_p(dd.data_ptr()), nb, ctypes.c_void_p(cot.data_ptr()), 1, 1,
                     ctypes.c_void_p(g.data_ptr()), st))
+            plan.reduce_shards(g)
             rows = torch.as_tensor(ctx.bas[:, 0].astype(np.int64), device=d.device)
             owner = torch.as_tensor(basis.shell_atoms.astype(np.int64), device=d.device)
             grad_c = torch.zeros((ctx.natom, 3), dtype=torch.float64, device=d.device)

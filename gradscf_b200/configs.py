@@ -156,9 +156,10 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("config", choices=("c0", "c2", "c3", "c4"))
     ap.add_argument("--quick", action="store_true", help="reduced size (smoke run)")
+    ap.add_argument("--cycles", type=int, default=15, help="c4: SCF iterations per precision")
     a = ap.parse_args(argv)
     fn = {"c0": run_c0, "c2": run_c2, "c3": lambda: run_c3(quick=a.quick),
-          "c4": lambda: run_c4(quick=a.quick)}[a.config]
+          "c4": lambda: run_c4(cycles=a.cycles, quick=a.quick)}[a.config]
     if a.config == "c2" and a.quick:
         fn = lambda: run_c2(nwater=4)  # noqa: E731
     print(json.dumps(fn()))

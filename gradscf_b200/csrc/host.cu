@@ -401,6 +401,21 @@ static void upload(DevBuf& b, const void* src, size_t n) {
   if (n) CUDA_OK(cudaMemcpy(b.ptr, src, n, cudaMemcpyHostToDevice));
 }
 
+// Bra/ket class lists of a class pair: pair ids and per-position records.
+static void set_lists(JKArgs& a, const Plan& p, const ClassPairWork& W) {
+  const ClassList& X = p.classes[W.x];
+  const ClassList& Y = p.classes[W.y];
+  a.bra_pairs = X.d_pairs.as<int>();
+  a.ket_pairs = Y.d_pairs.as<int>();
+  a.bra_ra = X.d_ra.as<double4>();
+  a.bra_ab = X.d_ab.as<double4>();
+  a.bra_ix = X.d_ix.as<int4>();
+  a.ket_ra = Y.d_ra.as<double4>();
+  a.ket_ab = Y.d_ab.as<double4>();
+  a.ket_ix = Y.d_ix.as<int4>();
+  a.same_list = W.x == W.y;
+}
+
 static JKArgs base_args(const Plan& p) {
   JKArgs a{};
   a.sh_info = p.d_ws_info.as<int4>();
@@ -650,6 +665,18 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     }
     upload(L.d_pairs, ids.data(), ids.size() * sizeof(int));
     upload(L.d_q, L.q.data(), L.q.size() * sizeof(double));
+    std::vector<double4> ra(ids.size()), ab(ids.size());
+    std::vector<int4> ix(ids.size());
+    for (size_t i = 0; i < ids.size(); ++i) {
+      const int4 pi = p.pair_info[ids[i]];
+      const double4 a = p.ws_xyz[pi.x], b = p.ws_xyz[pi.y];
+      ra[i] = make_double4(a.x, a.y, a.z, (double)p.ws_info[pi.x].z);
+      ab[i] = make_double4(a.x - b.x, a.y - b.y, a.z - b.z, 0.0);
+      ix[i] = make_int4(pi.z, pi.w, p.ws_info[pi.x].x, p.ws_info[pi.y].x);
+    }
+    upload(L.d_ra, ra.data(), ra.size() * sizeof(double4));
+    upload(L.d_ab, ab.data(), ab.size() * sizeof(double4));
+    upload(L.d_ix, ix.data(), ix.size() * sizeof(int4));
   }
   // ---- work items per class pair (X >= Y)
   const auto& disp = dispatch();
@@ -693,6 +720,12 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
       if (W->nwork == 0) { delete W; continue; }
       upload(W->work, items.data(), items.size() * sizeof(int4));
       W->h_items = items;
+      W->all_items = items;
+      W->item_cost.resize(items.size());
+      for (size_t i = 0; i < items.size(); ++i) {
+        const int4 it = items[i];
+        W->item_cost[i] = (long long)p.pair_info[X.pairs[it.x]].w * (Y.npp_prefix[it.z] - Y.npp_prefix[it.y]);
+      }
       CUDA_OK(W->split.ensure(W->nwork * sizeof(int)));
       p.work.push_back(W);
     }
@@ -804,6 +837,7 @@ void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j,
     maxabs_kernel<<<592, 256, 0, st>>>(d_in, (long long)nb * p.out_stride, p.d_maxd.as<double>());
     CUDA_OK(cudaGetLastError());
     for (auto* W : p.work) {
+      if (W->nwork == 0) continue;  // nothing of this class pair on this shard
       split_kernel<<<(W->nwork + 127) / 128, 128, 0, st>>>(
           W->work.as<int4>(), p.classes[W->x].d_q.as<double>(), p.classes[W->y].d_q.as<double>(),
           p.d_maxd.as<double>(), fp32_cut, W->nwork, W->split.as<int>());
@@ -822,9 +856,9 @@ void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j,
   a.with_k = with_k;
   const auto& disp = dispatch();
   for (auto* W : p.work) {
+    if (W->nwork == 0) continue;
     const int cls = quartet_class(W->x, W->y);
-    a.bra_pairs = p.classes[W->x].d_pairs.as<int>();
-    a.ket_pairs = p.classes[W->y].d_pairs.as<int>();
+    set_lists(a, p, *W);
     a.work = W->work.as<int4>();
     a.nwork = W->nwork;
     a.split = W->split.as<int>();
@@ -1045,6 +1079,60 @@ int b200jk_direct_jk_tables(const int32_t* atm, int32_t natm, const int32_t* bas
   });
 }
 
+int b200jk_partition_items(const int64_t* cost, int64_t n, int32_t world, int32_t* owner) {
+  return guarded([&] {
+    if (n < 0 || world < 1 || (n > 0 && (!cost || !owner))) invalid("Invalid partition request");
+    long double total = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      if (cost[i] < 0) invalid("Negative work-item cost");
+      total += (long double)cost[i];
+    }
+    // contiguous blocks: item i goes to the rank that owns the midpoint of
+    // its cost interval in [0, total)
+    long double before = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      int r;
+      if (total > 0) r = (int)((before + 0.5L * (long double)cost[i]) * world / total);
+      else r = (int)((i * (int64_t)world) / n);
+      owner[i] = std::min(std::max(r, 0), world - 1);
+      before += (long double)cost[i];
+    }
+  });
+}
+
+int b200jk_plan_set_shard(b200jk_plan* plan, int32_t rank, int32_t world) {
+  return guarded([&] {
+    if (!plan) invalid("Invalid plan");
+    if (world < 1 || rank < 0 || rank >= world) invalid("Invalid shard (rank, world)");
+    Plan& p = *plan->p;
+    CUDA_OK(cudaSetDevice(p.device));
+    CUDA_OK(cudaDeviceSynchronize());
+    for (auto* W : p.work) {
+      const int64_t n = (int64_t)W->all_items.size();
+      std::vector<int32_t> owner(n);
+      if (b200jk_partition_items(W->item_cost.data(), n, world, owner.data()) != 0)
+        throw Failure{B200JK_INTERNAL, "work-item partition failed"};
+      std::vector<int4> mine;
+      long long q = 0, pq = 0;
+      for (int64_t i = 0; i < n; ++i) {
+        if (owner[i] != rank) continue;
+        const int4 it = W->all_items[i];
+        mine.push_back(it);
+        q += it.z - it.y;
+        pq += W->item_cost[i];
+      }
+      W->h_items = mine;
+      W->nwork = (int)mine.size();
+      W->quartets = q;
+      W->prim_quartets = pq;
+      if (!mine.empty())  // the buffer holds the full list, so it is never reallocated
+        CUDA_OK(cudaMemcpy(W->work.ptr, mine.data(), mine.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
+    p.shard_rank = rank;
+    p.shard_world = world;
+  });
+}
+
 int b200jk_plan_class_stats(const b200jk_plan* plan, int64_t* quartets, int64_t* prim_quartets) {
   return guarded([&] {
     if (!plan || !quartets || !prim_quartets) invalid("Invalid plan query");
@@ -1185,9 +1273,9 @@ int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_
     a.grad = d_grad;
     const auto& disp = dispatch();
     for (auto* W : p.work) {
+      if (W->nwork == 0) continue;
       const int cls = quartet_class(W->x, W->y);
-      a.bra_pairs = p.classes[W->x].d_pairs.as<int>();
-      a.ket_pairs = p.classes[W->y].d_pairs.as<int>();
+      set_lists(a, p, *W);
       a.work = W->work.as<int4>();
       a.nwork = W->nwork;
       a.split_mode = 0;

@@ -32,6 +32,11 @@ struct JKArgs {
   const int* mol_n;          // Cartesian AO count of the molecule
   const int* bra_pairs;      // sorted pair ids of the bra class
   const int* ket_pairs;      // sorted pair ids of the ket class
+  // per list position: (Ax, Ay, Az, molecule), A - B, (first primitive
+  // pair, count, Cartesian offset of A, of B); same_list: bra list == ket list
+  const double4 *bra_ra, *bra_ab, *ket_ra, *ket_ab;
+  const int4 *bra_ix, *ket_ix;
+  int same_list;
   const int4* work;          // (bra position, ket begin, ket end, unused)
   int nwork;
   const int* split;          // per work item: first ket computed in FP32
@@ -108,6 +113,39 @@ __device__ __forceinline__ void load_quartet(const JKArgs& args, int bra, int ke
   if (g.A == g.B) s *= 0.5;
   if (g.C == g.D) s *= 0.5;
   if (bra == ket) s *= 0.5;
+  g.scale = s;
+}
+
+// Bra side of a work item from the per-position records (loaded once per warp).
+struct BraRec {
+  double4 ra, ab;
+  int4 ix;
+  int pos;
+};
+
+__device__ __forceinline__ BraRec load_bra(const JKArgs& args, int pos) {
+  return BraRec{args.bra_ra[pos], args.bra_ab[pos], args.bra_ix[pos], pos};
+}
+
+// Quartet from the bra record and the ket at list position kpos: three
+// coalesced loads per lane, no dependent table lookups.  The shell ids
+// A..D are not filled (the J/K paths address by Cartesian offset).
+__device__ __forceinline__ void load_quartet_rec(const JKArgs& args, const BraRec& b, int kpos,
+                                                 QuartetGeom& g) {
+  const double4 rc = args.ket_ra[kpos], cd = args.ket_ab[kpos];
+  const int4 kx = args.ket_ix[kpos];
+  g.A = g.B = g.C = g.D = -1;
+  g.ppa = b.ix.x; g.npa = b.ix.y; g.ppc = kx.x; g.npc = kx.y;
+  g.ax = b.ra.x; g.ay = b.ra.y; g.az = b.ra.z;
+  g.cx = rc.x; g.cy = rc.y; g.cz = rc.z;
+  g.abx = b.ab.x; g.aby = b.ab.y; g.abz = b.ab.z;
+  g.cdx = cd.x; g.cdy = cd.y; g.cdz = cd.z;
+  g.aoA = b.ix.z; g.aoB = b.ix.w; g.aoC = kx.z; g.aoD = kx.w;
+  g.mol = (int)b.ra.w;
+  double s = 1.0;
+  if (b.ix.z == b.ix.w) s *= 0.5;
+  if (kx.z == kx.w) s *= 0.5;
+  if (args.same_list && kpos == b.pos) s *= 0.5;
   g.scale = s;
 }
 
@@ -236,6 +274,10 @@ __device__ __forceinline__ long long dm_index(const JKArgs& args, int mol, int a
 // ---------------------------------------------------------------------------
 // Register path: one thread per quartet, the whole Cartesian block in registers.
 // ---------------------------------------------------------------------------
+#ifndef B200JK_REG_UNROLL
+#define B200JK_REG_UNROLL 2
+#endif
+constexpr int kRegUnroll = B200JK_REG_UNROLL;   // bra primitives interleaved per step (ILP)
 template <int LA, int LB, int LC, int LD, typename R>
 __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const QuartetGeom& g,
                                                   const typename PrimData<R>::A* bpp,
@@ -249,9 +291,17 @@ __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const Quar
   // ket primitive in registers (outer), bra primitives broadcast from
   // shared memory (inner): one global read per ket primitive pair.
   const float3 ac = make_float3(float(g.ax - g.cx), float(g.ay - g.cy), float(g.az - g.cz));
+  // the next ket primitive is fetched while the current one is in use
+  auto Qn = PrimData<R>::a(args, g.ppc);
+  auto QAn = PrimData<R>::b(args, g.ppc);
   for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
-    const auto Q = PrimData<R>::a(args, j);
-    const auto QA = PrimData<R>::b(args, j);
+    const auto Q = Qn;
+    const auto QA = QAn;
+    if (j + 1 < g.ppc + g.npc) {
+      Qn = PrimData<R>::a(args, j + 1);
+      QAn = PrimData<R>::b(args, j + 1);
+    }
+#pragma unroll(kRegUnroll)
     for (int i = 0; i < g.npa; ++i) {
       PrimQ<R> s;
       prim_any<R>(g, ac, bpp[i], baux[i], Q, QA, s);
@@ -285,13 +335,69 @@ __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const Quar
   }
 }
 
+// Density elements one quartet digests, in a fixed order: D[c][d] (J of the
+// bra), D[a][b] (J of the ket), then D[b][d], D[b][c], D[a][d], D[a][c] (the
+// four exchange terms).  Small classes fetch them into registers before the
+// primitive loop so the loads overlap the integral evaluation.
+template <int LA, int LB, int LC, int LD>
+struct DigestMap {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  static constexpr int NA = CI::NA, NB = CI::NB, NC = CI::NC, ND = CI::ND;
+  static constexpr int OJ1 = 0, OJ2 = NC * ND, OK1 = OJ2 + NA * NB, OK2 = OK1 + NB * ND,
+                       OK3 = OK2 + NB * NC, OK4 = OK3 + NA * ND, TOTAL = OK4 + NA * NC;
+};
+
+#ifndef B200JK_PRELOAD_MAX
+#define B200JK_PRELOAD_MAX 0   // measured on (H2O)32 cc-pVDZ: no gain from preloading
+#endif
+
+template <int LA, int LB, int LC, int LD, typename R>
+struct DensPre {
+  using M = DigestMap<LA, LB, LC, LD>;
+  static constexpr bool ON = M::TOTAL <= B200JK_PRELOAD_MAX;
+  R v[ON ? M::TOTAL : 1];
+  __device__ __forceinline__ void load(const JKArgs& args, const QuartetGeom& g) {
+    if constexpr (ON) {
+      const R* dm = DensSel<R>::get(args) + args.mol_base[g.mol];
+      const int n = args.mol_n[g.mol];
+      auto at = [&](int r, int c) { return __ldg(dm + (long long)r * n + c); };
+#pragma unroll
+      for (int c = 0; c < M::NC; ++c)
+#pragma unroll
+        for (int d = 0; d < M::ND; ++d) v[M::OJ1 + c * M::ND + d] = at(g.aoC + c, g.aoD + d);
+#pragma unroll
+      for (int a = 0; a < M::NA; ++a)
+#pragma unroll
+        for (int b = 0; b < M::NB; ++b) v[M::OJ2 + a * M::NB + b] = at(g.aoA + a, g.aoB + b);
+#pragma unroll
+      for (int b = 0; b < M::NB; ++b) {
+#pragma unroll
+        for (int d = 0; d < M::ND; ++d) v[M::OK1 + b * M::ND + d] = at(g.aoB + b, g.aoD + d);
+#pragma unroll
+        for (int c = 0; c < M::NC; ++c) v[M::OK2 + b * M::NC + c] = at(g.aoB + b, g.aoC + c);
+      }
+#pragma unroll
+      for (int a = 0; a < M::NA; ++a) {
+#pragma unroll
+        for (int d = 0; d < M::ND; ++d) v[M::OK3 + a * M::ND + d] = at(g.aoA + a, g.aoD + d);
+#pragma unroll
+        for (int c = 0; c < M::NC; ++c) v[M::OK4 + a * M::NC + c] = at(g.aoA + a, g.aoC + c);
+      }
+    }
+  }
+};
+
 // J[a][b] of the block's bra pair for density 0 goes to `jab` (reduced by
 // the caller) when acc_j is set; everything else is an atomic add.  Density
-// elements are read where they are used (L1/L2 resident).
+// elements come from `pre` (density 0 of small classes) or are read where
+// they are used (L1/L2 resident).
 template <int LA, int LB, int LC, int LD, typename R>
 __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom& g, const R* out,
-                                           bool acc_j, bool active, double* s_jab_row) {
+                                           bool acc_j, bool active, double* s_jab_row,
+                                           const DensPre<LA, LB, LC, LD, R>& pre) {
   using CI = ClassInfo<LA, LB, LC, LD>;
+  using M = DigestMap<LA, LB, LC, LD>;
+  constexpr bool PRE = DensPre<LA, LB, LC, LD, R>::ON;
   constexpr int NA = CI::NA, NB = CI::NB, NC = CI::NC, ND = CI::ND;
   const double s = g.scale;
   const long long base = args.mol_base[g.mol];
@@ -302,6 +408,13 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
 #define V_(a, b, c, d) (out[(((a) * NB + (b)) * NC + (c)) * ND + (d)])
   for (int e = 0; e < args.ndm; ++e) {
     const R* dm = dens + e * args.dstride + base;
+    const bool use_pre = PRE && e == 0;
+    auto dv = [&](int slot, int r, int c) -> R {
+      if constexpr (PRE) {
+        if (use_pre) return pre.v[slot];
+      }
+      return __ldg(dm + (long long)r * n + c);
+    };
     if (args.with_j && e < args.nsym) {
       double* vj = args.vj + e * args.dstride + base;
 #pragma unroll
@@ -312,7 +425,7 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
 #pragma unroll
           for (int c = 0; c < NC; ++c)
 #pragma unroll
-            for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoC + c) * n + g.aoD + d);
+            for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * dv(M::OJ1 + c * ND + d, g.aoC + c, g.aoD + d);
           if (acc_j && e == 0) {
             // bra-block J of density 0: warp-reduced here, added once per work item
             double v = active ? 2.0 * s * double(acc) : 0.0;
@@ -331,7 +444,7 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
 #pragma unroll
           for (int a = 0; a < NA; ++a)
 #pragma unroll
-            for (int b = 0; b < NB; ++b) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoA + a) * n + g.aoB + b);
+            for (int b = 0; b < NB; ++b) acc += V_(a, b, c, d) * dv(M::OJ2 + a * NB + b, g.aoA + a, g.aoB + b);
           if (active) atomicAdd(vj + (long long)(g.aoC + c) * n + g.aoD + d, 2.0 * s * double(acc));
         }
     }
@@ -345,7 +458,7 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
 #pragma unroll
           for (int b = 0; b < NB; ++b)
 #pragma unroll
-            for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoB + b) * n + g.aoD + d);
+            for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * dv(M::OK1 + b * ND + d, g.aoB + b, g.aoD + d);
           if (active) atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoC + c, s * double(acc));
         }
 #pragma unroll
@@ -356,7 +469,7 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
 #pragma unroll
           for (int b = 0; b < NB; ++b)
 #pragma unroll
-            for (int c = 0; c < NC; ++c) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoB + b) * n + g.aoC + c);
+            for (int c = 0; c < NC; ++c) acc += V_(a, b, c, d) * dv(M::OK2 + b * NC + c, g.aoB + b, g.aoC + c);
           if (active) atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoD + d, s * double(acc));
         }
 #pragma unroll
@@ -367,7 +480,7 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
 #pragma unroll
           for (int a = 0; a < NA; ++a)
 #pragma unroll
-            for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoA + a) * n + g.aoD + d);
+            for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * dv(M::OK3 + a * ND + d, g.aoA + a, g.aoD + d);
           if (active) atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoC + c, s * double(acc));
         }
 #pragma unroll
@@ -378,7 +491,7 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
 #pragma unroll
           for (int a = 0; a < NA; ++a)
 #pragma unroll
-            for (int c = 0; c < NC; ++c) acc += V_(a, b, c, d) * __ldg(dm + (long long)(g.aoA + a) * n + g.aoC + c);
+            for (int c = 0; c < NC; ++c) acc += V_(a, b, c, d) * dv(M::OK4 + a * NC + c, g.aoA + a, g.aoC + c);
           if (active) atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoD + d, s * double(acc));
         }
     }
@@ -393,7 +506,11 @@ struct RegMinBlocks {
   // estimated live registers: output block + one root's 2D integrals + ~70 for
   // addresses, primitive scalars and digestion (FP64 values take two)
   static constexpr int EST = (sizeof(R) == 8 ? 2 : 1) * (CI::NOUT + 3 * CI::NG) + 70;
-  static constexpr int value = EST <= 84 ? 6 : (EST <= 100 ? 5 : (EST <= 124 ? 4 : (EST <= 160 ? 3 : 2)));
+  static constexpr int base = EST <= 84 ? 6 : (EST <= 100 ? 5 : (EST <= 124 ? 4 : (EST <= 160 ? 3 : 2)));
+#ifndef B200JK_MINB_DELTA
+#define B200JK_MINB_DELTA 0
+#endif
+  static constexpr int value = base + B200JK_MINB_DELTA < 1 ? 1 : base + B200JK_MINB_DELTA;
 };
 
 constexpr int kBraPrimCache = 64;
@@ -432,40 +549,42 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
     else kb = max(kb, sp);
   }
   if (kb >= ke) return;
-  const int bra = args.bra_pairs[w.x];
-  const int4 pb = args.pair_info[bra];
-  const bool cached = pb.w <= kBraPrimCache;
+  const BraRec br = load_bra(args, w.x);
+  const int ppb = br.ix.x, npb = br.ix.y;
+  const bool cached = npb <= kBraPrimCache;
   if (cached)
-    for (int i = lane; i < pb.w; i += 32) {
-      s_pp[warp][i] = PrimData<R>::a(args, pb.z + i);
-      s_aux[warp][i] = PrimData<R>::b(args, pb.z + i);
+    for (int i = lane; i < npb; i += 32) {
+      s_pp[warp][i] = PrimData<R>::a(args, ppb + i);
+      s_aux[warp][i] = PrimData<R>::b(args, ppb + i);
     }
   const bool acc_j = args.with_j && args.nsym == 1;
   for (int i = lane; i < CI::NAB; i += 32) s_jab[warp][i] = 0.0;
   __syncwarp();
-  const PA_t* bpp = cached ? s_pp[warp] : (sizeof(R) == 4 ? (const PA_t*)(args.pp_f + pb.z)
-                                                         : (const PA_t*)(args.pp_data + pb.z));
-  const PB_t* baux = cached ? s_aux[warp] : (sizeof(R) == 4 ? (const PB_t*)(args.pp_f2 + pb.z)
-                                                           : (const PB_t*)(args.pp_aux + pb.z));
+  const PA_t* bpp = cached ? s_pp[warp] : (sizeof(R) == 4 ? (const PA_t*)(args.pp_f + ppb)
+                                                         : (const PA_t*)(args.pp_data + ppb));
+  const PB_t* baux = cached ? s_aux[warp] : (sizeof(R) == 4 ? (const PB_t*)(args.pp_f2 + ppb)
+                                                           : (const PB_t*)(args.pp_aux + ppb));
   QuartetGeom g;
   for (int k0 = kb; k0 < ke; k0 += 32) {
     // lanes past the range recompute the last ket with their output masked,
     // so the whole warp takes part in the J shuffles
     const bool active = k0 + lane < ke;
     const int k = active ? k0 + lane : ke - 1;
-    load_quartet(args, bra, args.ket_pairs[k], g);
+    load_quartet_rec(args, br, k, g);
+    DensPre<LA, LB, LC, LD, R> pre;
+    pre.load(args, g);
     R out[CI::NOUT];
     quartet_block_reg<LA, LB, LC, LD, R>(args, g, bpp, baux, out, s_boys);
-    digest_reg<LA, LB, LC, LD, R>(args, g, out, acc_j, active, s_jab[warp]);
+    digest_reg<LA, LB, LC, LD, R>(args, g, out, acc_j, active, s_jab[warp], pre);
   }
   if (acc_j) {
     __syncwarp();
-    const int4 ia = args.sh_info[pb.x], ib = args.sh_info[pb.y];
-    double* vj = args.vj + args.mol_base[ia.z];
-    const int n = args.mol_n[ia.z];
+    const int mol = (int)br.ra.w;
+    double* vj = args.vj + args.mol_base[mol];
+    const int n = args.mol_n[mol];
     for (int ab = lane; ab < CI::NAB; ab += 32) {
       const double v = s_jab[warp][ab];
-      if (v != 0.0) atomicAdd(vj + (long long)(ia.x + ab / CI::NB) * n + ib.x + ab % CI::NB, v);
+      if (v != 0.0) atomicAdd(vj + (long long)(br.ix.z + ab / CI::NB) * n + br.ix.w + ab % CI::NB, v);
     }
   }
 }
@@ -658,10 +777,10 @@ __global__ void jk_team_kernel(JKArgs args) {
   const int4 w = args.work[blockIdx.x];
   int kb, ke;
   ket_range(args, w, kb, ke);
-  const int bra = args.bra_pairs[w.x];
+  const BraRec br = load_bra(args, w.x);
   for (int k = kb + team; k < ke; k += nteams) {
     QuartetGeom g;
-    load_quartet(args, bra, args.ket_pairs[k], g);
+    load_quartet_rec(args, br, k, g);
     team_block<LA, LB, LC, LD, R, TEAM>(args, g, sm, vsm, lane, mask);
     team_digest<LA, LB, LC, LD, TEAM>(args, g, vsm, lane);
     __syncwarp(mask);
@@ -707,7 +826,7 @@ __global__ void __launch_bounds__(128) jk_tile_kernel(JKArgs args) {
   R* G = reinterpret_cast<R*>(smem_raw + (size_t)team * TC::SLOT);
   R* roots = G + 3 * N * NG;
   double* V = reinterpret_cast<double*>(smem_raw + (size_t)team * TC::SLOT + TC::G_BYTES);
-  const int bra = args.bra_pairs[w.x];
+  const BraRec br = load_bra(args, w.x);
   // this lane's bra Cartesian pair
   const int ia = lane / CI::NB, ib = lane % CI::NB;
   const int bx = GI::idx(cart_lx(LA, ia), cart_lx(LB, ib), 0, 0);
@@ -716,7 +835,7 @@ __global__ void __launch_bounds__(128) jk_tile_kernel(JKArgs args) {
   for (int k0 = kb; k0 < ke; k0 += TC::Q) {
     const bool active = k0 + team < ke;
     QuartetGeom g;
-    load_quartet(args, bra, args.ket_pairs[active ? k0 + team : ke - 1], g);
+    load_quartet_rec(args, br, active ? k0 + team : ke - 1, g);
     R acc[CI::NCD];
 #pragma unroll
     for (int q = 0; q < CI::NCD; ++q) acc[q] = R(0);

@@ -41,7 +41,9 @@ struct ClassPairWork {
   DevBuf split;                 // int per work item: first FP32 ket (filled per call)
   long long quartets = 0;       // significant work-shell quartets in this class pair
   long long prim_quartets = 0;  // their primitive quartets
-  std::vector<int4> h_items;    // host copy of the work items
+  std::vector<int4> h_items;    // host copy of the active work items (this rank's shard)
+  std::vector<int4> all_items;  // every work item of the class pair
+  std::vector<int64_t> item_cost;  // primitive quartets per item (all_items order)
 };
 
 struct ClassList {
@@ -51,6 +53,10 @@ struct ClassList {
   std::vector<std::vector<int2>> segs;  // per molecule: [begin, end) runs of equal primitive-pair count
   std::vector<long long> npp_prefix;  // prefix sums of primitive-pair counts (size+1)
   DevBuf d_pairs, d_q;
+  // per list position (coalesced reads by consecutive kets): centre A and
+  // molecule (Ax, Ay, Az, mol), A - B, and (first primitive pair, count,
+  // Cartesian offset of A, of B) in the molecule
+  DevBuf d_ra, d_ab, d_ix;
 };
 
 struct ProfileEvent {
@@ -61,6 +67,7 @@ struct ProfileEvent {
 
 struct Plan {
   int device = 0;
+  int shard_rank = 0, shard_world = 1;  // active work-item shard
   int cart = 0;
   double cutoff = 0.0;
   int nmol = 0;

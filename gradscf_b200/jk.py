@@ -26,6 +26,14 @@ PRECISIONS = {"fp64": _capi.FP64, "split": _capi.SPLIT}
 DEFAULT_FP32_CUT = 1e-6
 
 
+def allreduce_partial(out, group=None):
+    """Sum the ranks' partial J/K (or gradient) in place: one all-reduce
+    over `group` (NCCL for CUDA tensors, gloo for CPU tensors)."""
+    import torch.distributed as dist
+    dist.all_reduce(out, op=dist.ReduceOp.SUM, group=group)
+    return out
+
+
 def _stream_handle(stream=None):
     s = stream if stream is not None else torch.cuda.current_stream()
     return ctypes.c_void_p(s.cuda_stream)
@@ -75,6 +83,25 @@ class DirectJKPlan:
         q = ctypes.c_int64()
         _capi.check(lib.b200jk_plan_quartets(self._h, ctypes.byref(q)))
         self.quartets = q.value
+        self.shard = (0, 1)
+        self.group = None
+
+    def set_shard(self, rank, world, group=None):
+        """Evaluate only shard `rank` of `world` (contiguous cost-balanced
+        blocks of every class pair's work items; ``b200jk_plan_set_shard``).
+        Results of ``jk_packed`` / ``JKGraph.run`` are then summed over the
+        ranks of `group` (one ``torch.distributed`` all-reduce, NCCL on GPUs)
+        unless ``reduce=False`` is passed; ``(0, 1)`` restores the whole build."""
+        with torch.cuda.device(self.device):
+            _capi.check(_capi.lib().b200jk_plan_set_shard(self._h, int(rank), int(world)))
+        self.shard = (int(rank), int(world))
+        self.group = group
+
+    def reduce_shards(self, out):
+        """Sum a sharded result over the ranks (in place); no-op when unsharded."""
+        if self.shard[1] > 1:
+            allreduce_partial(out, self.group)
+        return out
 
     def close(self):
         if getattr(self, "_h", None):
@@ -89,8 +116,9 @@ class DirectJKPlan:
 
     # -- J/K ---------------------------------------------------------------
     def jk_packed(self, density, *, with_j=True, with_k=True, hermi=0, precision="fp64",
-                  fp32_cut=DEFAULT_FP32_CUT, out=None, stream=None, check=True):
-        """density: (nb, packed_size) float64 CUDA tensor -> (nops, nb, packed_size)."""
+                  fp32_cut=DEFAULT_FP32_CUT, out=None, stream=None, check=True, reduce=True):
+        """density: (nb, packed_size) float64 CUDA tensor -> (nops, nb, packed_size).
+        On a sharded plan the partial results are all-reduced when `reduce`."""
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
         d = density
@@ -109,6 +137,8 @@ class DirectJKPlan:
                 float(fp32_cut), st))
             if check:
                 _capi.check(_capi.lib().b200jk_check_status(self._h, st))
+        if reduce:
+            self.reduce_shards(out)
         return out
 
     def jk(self, density, *, with_j=True, with_k=True, hermi=None, precision="fp64",
@@ -153,10 +183,16 @@ class JKGraph:
                 float(fp32_cut), ctypes.byref(h)))
         self._h = h
 
-    def run(self, density, stream=None):
+    def run(self, density, stream=None, reduce=True):
         self.inp.copy_(density.reshape(self.inp.shape))
+        return self.launch(stream, reduce)
+
+    def launch(self, stream=None, reduce=True):
+        """Replay on the current contents of ``self.inp``."""
         with torch.cuda.device(self.plan.device):
             _capi.check(_capi.lib().b200jk_graph_launch(self._h, _stream_handle(stream)))
+        if reduce:
+            self.plan.reduce_shards(self.out)
         return self.out
 
     def close(self):

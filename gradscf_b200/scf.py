@@ -193,6 +193,7 @@ def rhf_gradient(mol: Molecule, res: SCFResult):
         _capi.check(lib.b200jk_direct_jk_geom_vjp(mol.plan._h, ctypes.c_void_p(dd.data_ptr()), 1,
                                                   ctypes.c_void_p(cot.data_ptr()), 1, 1,
                                                   ctypes.c_void_p(g2.data_ptr()), st))
+    mol.plan.reduce_shards(g2)   # sharded plan: sum the ranks' two-electron parts
     g = (g1 + g2).cpu().numpy()
     nnuc = len(mol.charges)
     out = g[:nnuc].copy()

@@ -74,6 +74,18 @@ int b200jk_plan_block_offsets(const b200jk_plan* plan, int64_t* offsets);
  * split-contraction shells and their primitive quartets.  For the FLOP model. */
 int b200jk_plan_class_stats(const b200jk_plan* plan, int64_t* quartets, int64_t* prim_quartets);
 
+/* Multi-GPU sharding of one J/K build (replaces the reference's per-process
+ * row-range worker ownership, csrc/direct_jk.cc:26-92, across devices).
+ * b200jk_partition_items: host-only; assigns n work items with the given
+ * costs to `world` ranks in contiguous, cost-balanced blocks (owner[i] in
+ * [0, world)).  b200jk_plan_set_shard: from now on the plan evaluates only
+ * rank `rank`'s items of every class pair (costs = primitive quartets), so
+ * the J/K it returns is this rank's partial sum; the caller sums the ranks'
+ * outputs (one all-reduce).  (0, 1) restores the whole build.  Graphs
+ * created before the call keep the shard they captured. */
+int b200jk_partition_items(const int64_t* cost, int64_t n, int32_t world, int32_t* owner);
+int b200jk_plan_set_shard(b200jk_plan* plan, int32_t rank, int32_t world);
+
 /* After a B200JK_SPLIT call (synchronises `stream`): per class pair, the
  * quartets and primitive quartets that ran in FP64 and in FP32. */
 int b200jk_plan_split_stats(b200jk_plan* plan, void* stream, int64_t* q64, int64_t* q32,

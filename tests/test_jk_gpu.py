@@ -152,3 +152,27 @@ def test_quartet_count_matches_oracle():
     plan = J.cached_plan(atm, bas, env, cart=False, cutoff=1e-12)
     q = oracle.schwarz_bounds(atm, bas, env, cart=False)
     assert plan.quartets == oracle.count_quartets(q, 1e-12)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_sharded_partials_sum_to_full_build(precision):
+    # the shards of a 3-way split, run one after another on this GPU, add up
+    # to the unsharded build (the multi-GPU path sums them with one all-reduce)
+    from gradscf_b200 import workloads as W
+    top, par, sa, atm, bas, env = tables(W.water_cluster(3, 1), "cc-pvdz", False)
+    plan = J.DirectJKPlan([(atm, bas, env)], cart=False, cutoff=1e-12)
+    n = plan.nao[0]
+    d = torch.as_tensor(psd_density(n, 15, 4), device="cuda").reshape(1, -1)
+    full = plan.jk_packed(d, hermi=1, precision=precision).clone()
+    acc = torch.zeros_like(full)
+    nonempty = 0
+    for r in range(3):
+        plan.set_shard(r, 3)
+        part = plan.jk_packed(d, hermi=1, precision=precision, reduce=False)
+        nonempty += int(part.abs().max().item() > 0)
+        acc += part
+    plan.set_shard(0, 1)
+    assert nonempty == 3
+    assert (acc - full).abs().max().item() < 1e-11
+    again = plan.jk_packed(d, hermi=1, precision=precision)
+    assert (again - full).abs().max().item() < 1e-12
