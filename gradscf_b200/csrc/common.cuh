@@ -62,7 +62,9 @@ template <> __device__ __forceinline__ double dexp<double>(double x) { return ex
 template <> __device__ __forceinline__ float dexp<float>(float x) { return __expf(x); }
 template <typename R> __device__ __forceinline__ R dsqrt(R x);
 template <> __device__ __forceinline__ double dsqrt<double>(double x) { return sqrt(x); }
-template <> __device__ __forceinline__ float dsqrt<float>(float x) { return sqrtf(x); }
+// FP32 quartets need ~1e-7 relative accuracy: hardware approximations (a
+// few ulp) instead of the IEEE-rounded sequences; arguments are positive.
+template <> __device__ __forceinline__ float dsqrt<float>(float x) { return x * rsqrtf(x); }
 template <typename R> __device__ __forceinline__ R drsqrt(R x);
 template <> __device__ __forceinline__ double drsqrt<double>(double x) { return rsqrt(x); }
 template <> __device__ __forceinline__ float drsqrt<float>(float x) { return rsqrtf(x); }
@@ -138,7 +140,7 @@ __device__ __forceinline__ void boys_fn(R t, R* f, const R* tab) {
 
 template <typename R> __device__ __forceinline__ R drcp(R x);
 template <> __device__ __forceinline__ double drcp<double>(double x) { return 1.0 / x; }
-template <> __device__ __forceinline__ float drcp<float>(float x) { return __frcp_rn(x); }
+template <> __device__ __forceinline__ float drcp<float>(float x) { return __fdividef(1.0f, x); }
 
 // Rys nodes x_i = t_i^2 and weights w_i for N <= 3 from the Boys moments
 // mu_k = F_k(T) (k < 2N): Gautschi's Chebyshev algorithm gives the Jacobi
@@ -196,8 +198,8 @@ __device__ __forceinline__ void rys_small(R t, R* x, R* w, const R* tab) {
     const R d0 = a0 - m, d1 = a1 - m, d2 = a2 - m;
     const R p = R(-0.5) * (d0 * d0 + d1 * d1 + d2 * d2 + R(2) * (b1 + b2));
     const R q = -(d0 * d1 * d2 - d0 * b2 - d2 * b1);
-    const float r = sqrtf(float(-p) * (1.0f / 3.0f));
-    const float cth = fminf(fmaxf(-float(q) / (2.0f * r * r * r), -1.0f), 1.0f);
+    const float r = dsqrt<float>(float(-p) * (1.0f / 3.0f));
+    const float cth = fminf(fmaxf(__fdividef(-float(q), 2.0f * r * r * r), -1.0f), 1.0f);
     const float th = acosf(cth) * (1.0f / 3.0f);
     const R sb1 = dsqrt<R>(b1), sb2 = dsqrt<R>(b2);
     const R isb1 = drcp<R>(sb1), isb2 = drcp<R>(sb2);
@@ -258,7 +260,7 @@ __device__ __forceinline__ void rys_roots(R t, R* x, R* w, const Tables& tb) {
   }
   const int nint = tb.rys_nint[N];
   if (t >= R(nint)) {
-    const R rt = R(1) / t, rs = drsqrt<R>(t);
+    const R rt = drcp<R>(t), rs = drsqrt<R>(t);
 #pragma unroll
     for (int i = 0; i < N; ++i) {
       x[i] = R(tb.asym_r[N * 8 + i]) * rt;

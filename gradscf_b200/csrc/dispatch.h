@@ -19,7 +19,8 @@ struct DispatchTable {
   JKLauncher jk32[kQuartetClasses] = {};
   GradLauncher grad64[kQuartetClasses] = {};
   SchwarzLauncher schwarz[kPairClasses] = {};
-  bool reg_path[kQuartetClasses] = {};
+  bool reg_path[kQuartetClasses] = {};   // either precision runs the register path
+  bool tile[kQuartetClasses] = {};       // the FP64 kernel is the tile path
   int team[kQuartetClasses] = {};
 };
 

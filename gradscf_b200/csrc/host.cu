@@ -686,7 +686,11 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
       const ClassList& Y = p.classes[y];
       if (X.pairs.empty() || Y.pairs.empty()) continue;
       const int cls = quartet_class(x, y);
-      const int chunk = disp.reg_path[cls] ? 64 : std::max(8, 4 * (128 / disp.team[cls]));
+#ifndef B200JK_TILE_CHUNK
+#define B200JK_TILE_CHUNK 64   // kets per tile-path work item (measured best of 16/32/64)
+#endif
+      int chunk = disp.reg_path[cls] ? 64 : std::max(8, 4 * (128 / disp.team[cls]));
+      if (B200JK_TILE_CHUNK > 0 && disp.tile[cls]) chunk = B200JK_TILE_CHUNK;
       auto* W = new ClassPairWork();
       W->x = x;
       W->y = y;

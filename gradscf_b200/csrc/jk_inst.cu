@@ -18,10 +18,17 @@ constexpr int pc_lb(int pc) { return pc - pc_la(pc) * (pc_la(pc) + 1) / 2; }
 
 // Kernel shape policy: a register path for blocks that fit one thread,
 // otherwise a team whose lanes hold about 24 outputs each.
-template <int LA, int LB, int LC, int LD>
+#ifndef B200JK_REG_LIMIT32
+#define B200JK_REG_LIMIT32 240
+#endif
+template <int LA, int LB, int LC, int LD, typename R = double>
 struct Policy {
   using CI = ClassInfo<LA, LB, LC, LD>;
-  static constexpr bool REG = (3 * CI::NG + CI::NOUT <= 96) && CI::NROOT <= 3;
+  // FP32 blocks take half the registers of FP64 ones: a larger register-path
+  // limit (measured on (H2O)32 cc-pVDZ: (11|11), (21|11), (21|20), (22|10)
+  // run 3-6x faster there than on the tile path)
+  static constexpr int LIMIT = sizeof(R) == 4 ? B200JK_REG_LIMIT32 : 96;
+  static constexpr bool REG = (3 * CI::NG + CI::NOUT <= LIMIT) && CI::NROOT <= 3;
   // tile path: kets up to d x d (NCD <= 36), bra pair fits one block
   static constexpr bool TILE = !REG && CI::NCD <= 36 && CI::NAB <= 128;
   static constexpr int TEAM = CI::NOUT <= 4 * 24 ? 4 : CI::NOUT <= 8 * 24 ? 8 : CI::NOUT <= 16 * 24 ? 16 : 32;
@@ -30,7 +37,7 @@ struct Policy {
 template <int LA, int LB, int LC, int LD, typename R>
 int launch_class(const JKArgs& args, cudaStream_t stream) {
   if (args.nwork <= 0) return 0;
-  using P = Policy<LA, LB, LC, LD>;
+  using P = Policy<LA, LB, LC, LD, R>;
   if constexpr (P::REG) {
     jk_reg_kernel<LA, LB, LC, LD, R><<<(args.nwork + kRegWarps - 1) / kRegWarps, 32 * kRegWarps, 0, stream>>>(args);
   } else if constexpr (P::TILE) {
@@ -126,7 +133,8 @@ void REG_NAME(BRA_CLASS, KET_CLASS)(DispatchTable& t) {
   t.jk64[id] = &launch_class<XA, XB, YA, YB, double>;
   t.jk32[id] = &launch_class<XA, XB, YA, YB, float>;
   t.grad64[id] = &launch_grad<XA, XB, YA, YB>;
-  t.reg_path[id] = Policy<XA, XB, YA, YB>::REG;
+  t.reg_path[id] = Policy<XA, XB, YA, YB, float>::REG || Policy<XA, XB, YA, YB>::REG;
+  t.tile[id] = Policy<XA, XB, YA, YB>::TILE;
   t.team[id] = Policy<XA, XB, YA, YB>::REG ? 1
                : (Policy<XA, XB, YA, YB>::TILE ? TileCfg<XA, XB, YA, YB, double>::THREADS / 4
                                                : Policy<XA, XB, YA, YB>::TEAM);
