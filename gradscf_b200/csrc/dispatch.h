@@ -19,6 +19,11 @@ struct DispatchTable {
   JKLauncher jk32[kQuartetClasses] = {};
   GradLauncher grad64[kQuartetClasses] = {};
   SchwarzLauncher schwarz[kPairClasses] = {};
+  // grouped-list kernels by (bra, ket) combinations: slot 3*g(gb) + g(gk),
+  // g(1) = 0, g(2) = 1, g(4) = 2 (slot 0 is the plain kernel above)
+  JKLauncher jkg64[kQuartetClasses][9] = {};
+  JKLauncher jkg32[kQuartetClasses][9] = {};
+  bool grouped[kQuartetClasses] = {};    // the class pair takes grouped lists
   bool reg_path[kQuartetClasses] = {};   // either precision runs the register path
   bool tile[kQuartetClasses] = {};       // the FP64 kernel is the tile path
   int team[kQuartetClasses] = {};

@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <set>
 #include <functional>
 #include <memory>
 #include <mutex>
@@ -416,6 +417,50 @@ static void set_lists(JKArgs& a, const Plan& p, const ClassPairWork& W) {
   a.same_list = W.x == W.y;
 }
 
+// The J/K launches of one class pair: its buckets on grouped lists, or its
+// expanded work items.
+struct JKUnit {
+  const DevBuf* work;
+  int nwork;
+  DevBuf* split;
+  const ClassList* X;
+  const ClassList* Y;
+  int gb, gk;
+  std::vector<int4>* h_items;
+};
+
+template <typename F>
+static void for_each_unit(Plan& p, ClassPairWork& W, F&& f) {
+  if (!W.buckets.empty()) {
+    const ClassList* X = W.grouped_x ? &p.grouped[W.x] : &p.classes[W.x];
+    const ClassList* Y = W.grouped_y ? &p.grouped[W.y] : &p.classes[W.y];
+    for (auto* B : W.buckets) f(JKUnit{&B->work, B->nwork, &B->split, X, Y, B->gb, B->gk, &B->h_items});
+  } else {
+    f(JKUnit{&W.work, W.nwork, &W.split, &p.classes[W.x], &p.classes[W.y], 1, 1, &W.h_items});
+  }
+}
+
+static void set_unit_lists(JKArgs& a, const JKUnit& u, bool same) {
+  a.bra_pairs = u.X->d_pairs.as<int>();
+  a.ket_pairs = u.Y->d_pairs.as<int>();
+  a.bra_ra = u.X->d_ra.as<double4>();
+  a.bra_ab = u.X->d_ab.as<double4>();
+  a.bra_ix = u.X->d_ix.as<int4>();
+  a.bra_gx = u.X->d_gx.as<int4>();
+  a.bra_gy = u.X->d_gy.as<int4>();
+  a.ket_ra = u.Y->d_ra.as<double4>();
+  a.ket_ab = u.Y->d_ab.as<double4>();
+  a.ket_ix = u.Y->d_ix.as<int4>();
+  a.ket_gx = u.Y->d_gx.as<int4>();
+  a.ket_gy = u.Y->d_gy.as<int4>();
+  a.same_list = same;
+}
+
+static int gen_slot(int gb, int gk) {
+  auto k = [](int g) { return g == 1 ? 0 : (g == 2 ? 1 : 2); };
+  return k(gb) * 3 + k(gk);
+}
+
 static JKArgs base_args(const Plan& p) {
   JKArgs a{};
   a.sh_info = p.d_ws_info.as<int4>();
@@ -426,6 +471,8 @@ static JKArgs base_args(const Plan& p) {
   a.pp_exp = p.d_pp_exp.as<double2>();
   a.pp_f = p.d_pp_f.as<float4>();
   a.pp_f2 = p.d_pp_f2.as<float2>();
+  a.pp_c = p.d_pp_c.as<double4>();
+  a.pp_cf = p.d_pp_cf.as<float4>();
   a.ws_atm = p.d_ws_atm.as<int>();
   a.mol_base = p.d_mol_base_cart.as<long long>();
   a.mol_n = p.d_mol_ncart.as<int>();
@@ -433,6 +480,14 @@ static JKArgs base_args(const Plan& p) {
   a.status = p.d_status.as<int>();
   return a;
 }
+
+// One entry of a grouped list (pair classes (l, 0)): a parent shell pair
+// with nco contraction combinations (work shells ws[k] on A, wsb[k] on B).
+struct GenEntry {
+  int cls = 0, mol = 0, diag = 0, pair = -1, nco = 1, ppoff = 0, npp = 0;
+  int ws[4] = {0, 0, 0, 0}, wsb[4] = {0, 0, 0, 0};
+  std::pair<int, int> pkey;
+};
 
 static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double cut, int device) {
   if (nmol < 1 || !mols) invalid("At least one molecule is required");
@@ -534,6 +589,105 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     ws0 = wsn;
   }
   p.npair = (int)p.pair_info.size();
+  // every primitive pair of the expanded list carries its contraction
+  // coefficients inside K: combination coefficients (1, 0, 0, 0)
+  std::vector<double4> pp_c(pp_data.size(), make_double4(1.0, 0.0, 0.0, 0.0));
+  // ---- grouped entries (pair classes (l, 0)): one entry per parent shell
+  // pair carrying its contraction combinations, so primitive quartets shared
+  // by the combinations are evaluated once.  Entries with a single
+  // combination are the expanded pairs themselves.
+  std::map<std::pair<int, int>, int> ws_pair_id;
+  for (int q = 0; q < p.npair; ++q)
+    ws_pair_id[{std::max(p.pair_info[q].x, p.pair_info[q].y), std::min(p.pair_info[q].x, p.pair_info[q].y)}] = q;
+  std::vector<int> parent_ws0;  // first work shell of every parent shell
+  for (int w = 0; w < p.nws; ++w)
+    if (w == 0 || p.ws_parent[w] != p.ws_parent[w - 1]) parent_ws0.push_back(w);
+  std::vector<int> parent_nc(parent_ws0.size());
+  for (size_t i = 0; i < parent_ws0.size(); ++i)
+    parent_nc[i] = (i + 1 < parent_ws0.size() ? parent_ws0[i + 1] : p.nws) - parent_ws0[i];
+  std::vector<GenEntry> gen;
+  for (size_t pa = 0; pa < parent_ws0.size(); ++pa)
+    for (size_t pb = 0; pb <= pa; ++pb) {
+      int PA = (int)pa, PB = (int)pb;
+      const int la = p.ws_info[parent_ws0[PA]].y, lb = p.ws_info[parent_ws0[PB]].y;
+      if (p.ws_info[parent_ws0[PA]].z != p.ws_info[parent_ws0[PB]].z) continue;  // other molecule
+      if (lb > la) std::swap(PA, PB);
+      if (std::min(la, lb) != 0) continue;  // grouped lists hold pair classes (l, 0) only
+      const int nca = parent_nc[PA], ncb = parent_nc[PB];
+      GenEntry base{};
+      base.cls = pair_class(std::max(la, lb), 0);
+      base.mol = p.ws_info[parent_ws0[PA]].z;
+      base.diag = PA == PB;
+      base.pkey = std::make_pair(std::max(p.ws_parent[parent_ws0[PA]], p.ws_parent[parent_ws0[PB]]),
+                                 std::min(p.ws_parent[parent_ws0[PA]], p.ws_parent[parent_ws0[PB]]));
+      if (nca * ncb == 1) {
+        int A = parent_ws0[PA], B = parent_ws0[PB];
+        auto it = ws_pair_id.find({std::max(A, B), std::min(A, B)});
+        if (it == ws_pair_id.end()) continue;  // every primitive pair screened out
+        base.pair = it->second;
+        base.nco = 1;
+        const int4 pi = p.pair_info[base.pair];
+        base.ws[0] = pi.x;
+        base.wsb[0] = pi.y;
+        base.ppoff = pi.z;
+        base.npp = pi.w;
+        gen.push_back(base);
+        continue;
+      }
+      // ordered combinations (column of A, column of B), cut into runs of
+      // 4 (pair class (0,0)) or 2, then 2, then 1
+      std::vector<int2> combos;
+      for (int ca = 0; ca < nca; ++ca)
+        for (int cb = 0; cb < ncb; ++cb) combos.push_back(make_int2(ca, cb));
+      const int gmax = base.cls == 0 ? 4 : 2;
+      size_t c0 = 0;
+      while (c0 < combos.size()) {
+        const size_t rem = combos.size() - c0;
+        const int g = rem >= (size_t)gmax ? gmax : (rem >= 2 ? 2 : 1);
+        GenEntry e = base;
+        e.pair = -1;
+        e.nco = g;
+        const int A0 = parent_ws0[PA], B0 = parent_ws0[PB];
+        for (int k = 0; k < g; ++k) {
+          e.ws[k] = A0 + combos[c0 + k].x;
+          e.wsb[k] = B0 + combos[c0 + k].y;
+        }
+        const double4 ra = p.ws_xyz[A0], rb = p.ws_xyz[B0];
+        const double ab2 = (ra.x - rb.x) * (ra.x - rb.x) + (ra.y - rb.y) * (ra.y - rb.y) +
+                           (ra.z - rb.z) * (ra.z - rb.z);
+        e.ppoff = (int)pp_data.size();
+        for (int ia = 0; ia < p.ws_nprim[A0]; ++ia)
+          for (int ib = 0; ib < p.ws_nprim[B0]; ++ib) {
+            const double a = p.ws_exp[p.ws_prim_off[A0] + ia], b = p.ws_exp[p.ws_prim_off[B0] + ib];
+            const double pe = a + b;
+            const double expo = a * b / pe * ab2;
+            if (expo > 40.0) continue;
+            double c[4] = {0.0, 0.0, 0.0, 0.0};
+            bool any = false;
+            for (int k = 0; k < g; ++k) {
+              c[k] = p.ws_coef[p.ws_prim_off[e.ws[k]] + ia] * p.ws_coef[p.ws_prim_off[e.wsb[k]] + ib];
+              any = any || c[k] != 0.0;
+            }
+            if (!any) continue;
+            double kk = std::exp(-expo) / pe;
+            if (g == 1) {  // a lone combination keeps its coefficient in K
+              kk *= c[0];
+              c[0] = 1.0;
+            }
+            const double4 P = make_double4((a * ra.x + b * rb.x) / pe, (a * ra.y + b * rb.y) / pe,
+                                           (a * ra.z + b * rb.z) / pe, pe);
+            pp_data.push_back(P);
+            pp_aux.push_back(make_double2(kk, 0.5 / pe));
+            pp_exp.push_back(make_double2(a, b));
+            pp_f.push_back(make_float4(float(P.x - ra.x), float(P.y - ra.y), float(P.z - ra.z), float(pe)));
+            pp_f2.push_back(make_float2(float(kk), float(0.5 / pe)));
+            pp_c.push_back(make_double4(c[0], c[1], c[2], c[3]));
+          }
+        e.npp = (int)pp_data.size() - e.ppoff;
+        if (e.npp > 0) gen.push_back(e);
+        c0 += g;
+      }
+    }
   // ---- device upload
   upload(p.d_ws_info, p.ws_info.data(), p.ws_info.size() * sizeof(int4));
   upload(p.d_ws_xyz, p.ws_xyz.data(), p.ws_xyz.size() * sizeof(double4));
@@ -543,6 +697,13 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
   upload(p.d_pp_exp, pp_exp.data(), pp_exp.size() * sizeof(double2));
   upload(p.d_pp_f, pp_f.data(), pp_f.size() * sizeof(float4));
   upload(p.d_pp_f2, pp_f2.data(), pp_f2.size() * sizeof(float2));
+  {
+    std::vector<float4> pp_cf(pp_c.size());
+    for (size_t i = 0; i < pp_c.size(); ++i)
+      pp_cf[i] = make_float4(float(pp_c[i].x), float(pp_c[i].y), float(pp_c[i].z), float(pp_c[i].w));
+    upload(p.d_pp_c, pp_c.data(), pp_c.size() * sizeof(double4));
+    upload(p.d_pp_cf, pp_cf.data(), pp_cf.size() * sizeof(float4));
+  }
   upload(p.d_mol_base_cart, p.mol_cart_base.data(), nmol * sizeof(long long));
   upload(p.d_mol_ncart, p.mol_ncart.data(), nmol * sizeof(int));
   upload(p.d_mol_base_out, p.mol_out_base.data(), nmol * sizeof(long long));
@@ -650,6 +811,12 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     for (size_t i = 0; i < ids.size(); ++i) L.q[i] = p.pair_q[ids[i]];
     L.npp_prefix.assign(ids.size() + 1, 0);
     for (size_t i = 0; i < ids.size(); ++i) L.npp_prefix[i + 1] = L.npp_prefix[i] + p.pair_info[ids[i]].w;
+    L.npp_pos.resize(ids.size());
+    L.mol_pos.resize(ids.size());
+    for (size_t i = 0; i < ids.size(); ++i) {
+      L.npp_pos[i] = p.pair_info[ids[i]].w;
+      L.mol_pos[i] = p.ws_info[p.pair_info[ids[i]].x].z;
+    }
     L.mol_begin.assign(nmol + 1, 0);
     for (int q : ids) L.mol_begin[p.ws_info[p.pair_info[q].x].z + 1]++;
     for (int m = 0; m < nmol; ++m) L.mol_begin[m + 1] += L.mol_begin[m];
@@ -678,17 +845,128 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     upload(L.d_ab, ab.data(), ab.size() * sizeof(double4));
     upload(L.d_ix, ix.data(), ix.size() * sizeof(int4));
   }
+  // the combinations of the grouped entries cover exactly the expanded
+  // work pairs of their classes (checked once per plan, on the host)
+  {
+    std::vector<std::set<std::pair<int, int>>> want(kPairClasses), got(kPairClasses);
+    for (int q = 0; q < p.npair; ++q) {
+      const int c = p.pair_class[q];
+      if (c == 0 || c == 1 || c == 3 || c == 6)
+        want[c].insert({std::max(p.pair_info[q].x, p.pair_info[q].y), std::min(p.pair_info[q].x, p.pair_info[q].y)});
+    }
+    for (const GenEntry& e : gen)
+      for (int k = 0; k < e.nco; ++k) got[e.cls].insert({std::max(e.ws[k], e.wsb[k]), std::min(e.ws[k], e.wsb[k])});
+    for (int c = 0; c < kPairClasses; ++c)
+      for (const auto& wp : want[c])
+        if (!got[c].count(wp))
+          throw Failure{B200JK_INTERNAL, "grouped pair list misses a work pair of class " + std::to_string(c)};
+  }
+  // ---- grouped lists: same screening and order, plus the number of
+  // combinations (runs of equal (combinations, primitive pairs) per molecule)
+  for (int c = 0; c < kPairClasses; ++c) {
+    std::vector<int> ids;
+    bool any_gen = false;
+    for (size_t i = 0; i < gen.size(); ++i) {
+      if (gen[i].cls != c) continue;
+      const double q = std::sqrt(parent[gen[i].pkey]);
+      if (cut > 0 && q * qmax_mol[gen[i].mol] < cut) continue;
+      ids.push_back((int)i);
+      any_gen = any_gen || gen[i].nco > 1;
+    }
+    if (!any_gen) continue;  // identical to the expanded list
+    auto qof = [&](int i) { return std::sqrt(parent[gen[i].pkey]); };
+    std::sort(ids.begin(), ids.end(), [&](int a, int b) {
+      const GenEntry &ea = gen[a], &eb = gen[b];
+      if (ea.mol != eb.mol) return ea.mol < eb.mol;
+      if (ea.nco != eb.nco) return ea.nco < eb.nco;
+      if (ea.npp != eb.npp) return ea.npp < eb.npp;
+      const double qa = qof(a), qb = qof(b);
+      if (qa != qb) return qa > qb;
+      return a < b;
+    });
+    ClassList& L = p.grouped[c];
+    const size_t n = ids.size();
+    L.pairs.assign(n, -1);
+    L.q.resize(n);
+    L.nco.resize(n);
+    L.npp_pos.resize(n);
+    L.mol_pos.resize(n);
+    L.npp_prefix.assign(n + 1, 0);
+    std::vector<double4> ra(n), ab(n);
+    std::vector<int4> ix(n), gx(n), gy(n);
+    for (size_t i = 0; i < n; ++i) {
+      const GenEntry& e = gen[ids[i]];
+      L.pairs[i] = e.pair;
+      L.q[i] = qof(ids[i]);
+      L.nco[i] = e.nco;
+      L.npp_pos[i] = e.npp;
+      L.mol_pos[i] = e.mol;
+      L.npp_prefix[i + 1] = L.npp_prefix[i] + e.npp;
+      const double4 a = p.ws_xyz[e.ws[0]], b = p.ws_xyz[e.wsb[0]];
+      ra[i] = make_double4(a.x, a.y, a.z, (double)e.mol);
+      ab[i] = make_double4(a.x - b.x, a.y - b.y, a.z - b.z, 0.0);
+      int ao[4], bo[4];
+      for (int k = 0; k < 4; ++k) {
+        ao[k] = k < e.nco ? p.ws_info[e.ws[k]].x : 0;
+        bo[k] = k < e.nco ? p.ws_info[e.wsb[k]].x : 0;
+      }
+      const int diag = e.nco == 1 ? (ao[0] == bo[0]) : e.diag;
+      ix[i] = make_int4(e.ppoff, e.npp, ao[0], bo[0]);
+      gx[i] = make_int4(diag, 0, ao[1], bo[1]);
+      gy[i] = make_int4(ao[2], bo[2], ao[3], bo[3]);
+    }
+    L.mol_begin.assign(nmol + 1, 0);
+    for (size_t i = 0; i < n; ++i) L.mol_begin[L.mol_pos[i] + 1]++;
+    for (int m = 0; m < nmol; ++m) L.mol_begin[m + 1] += L.mol_begin[m];
+    L.segs.assign(nmol, {});
+    for (size_t i = 0; i < n;) {
+      size_t j = i + 1;
+      while (j < n && L.mol_pos[j] == L.mol_pos[i] && L.nco[j] == L.nco[i] && L.npp_pos[j] == L.npp_pos[i]) ++j;
+      L.segs[L.mol_pos[i]].push_back(make_int2((int)i, (int)j));
+      i = j;
+    }
+    upload(L.d_q, L.q.data(), n * sizeof(double));
+    upload(L.d_ra, ra.data(), n * sizeof(double4));
+    upload(L.d_ab, ab.data(), n * sizeof(double4));
+    upload(L.d_ix, ix.data(), n * sizeof(int4));
+    upload(L.d_gx, gx.data(), n * sizeof(int4));
+    upload(L.d_gy, gy.data(), n * sizeof(int4));
+  }
   // ---- work items per class pair (X >= Y)
   const auto& disp = dispatch();
+  // (bra position, ket run [lo, hi)) of every bra: the Schwarz-screened
+  // prefix of each ket run of the bra's molecule, canonical when X == Y
+  auto for_each_run = [&](const ClassList& X, const ClassList& Y, bool same, auto&& emit) {
+    for (int bp = 0; bp < (int)X.q.size(); ++bp) {
+      const int m = X.mol_pos[bp];
+      const double qb = X.q[bp];
+      for (const int2 seg : Y.segs[m]) {
+        const int lo = seg.x;
+        if (same && lo > bp) break;  // canonical: ket position <= bra position
+        int hi = seg.y;
+        if (cut > 0) {
+          int a = lo, b = seg.y;  // first ket with qb*qk < cut (bounds sorted descending)
+          while (a < b) {
+            const int mid = (a + b) >> 1;
+            if (qb * Y.q[mid] < cut) b = mid;
+            else a = mid + 1;
+          }
+          hi = a;
+        }
+        if (same) hi = std::min(hi, bp + 1);
+        if (hi > lo) emit(bp, lo, hi);
+      }
+    }
+  };
+#ifndef B200JK_TILE_CHUNK
+#define B200JK_TILE_CHUNK 64   // kets per tile-path work item (measured best of 16/32/64)
+#endif
   for (int x = 0; x < kPairClasses; ++x)
     for (int y = 0; y <= x; ++y) {
       const ClassList& X = p.classes[x];
       const ClassList& Y = p.classes[y];
       if (X.pairs.empty() || Y.pairs.empty()) continue;
       const int cls = quartet_class(x, y);
-#ifndef B200JK_TILE_CHUNK
-#define B200JK_TILE_CHUNK 64   // kets per tile-path work item (measured best of 16/32/64)
-#endif
       int chunk = disp.reg_path[cls] ? 64 : std::max(8, 4 * (128 / disp.team[cls]));
       if (B200JK_TILE_CHUNK > 0 && disp.tile[cls]) chunk = B200JK_TILE_CHUNK;
       auto* W = new ClassPairWork();
@@ -696,41 +974,55 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
       W->y = y;
       W->nbra = (int)X.pairs.size();
       std::vector<int4> items;
-      for (int bp = 0; bp < W->nbra; ++bp) {
-        const int m = p.ws_info[p.pair_info[X.pairs[bp]].x].z;
-        const double qb = X.q[bp];
-        const long long npa = p.pair_info[X.pairs[bp]].w;
-        for (const int2 seg : Y.segs[m]) {
-          const int lo = seg.x;
-          if (x == y && lo > bp) break;  // canonical: ket position <= bra position
-          int hi = seg.y;
-          if (cut > 0) {
-            int a = lo, b = seg.y;  // first ket with qb*qk < cut (bounds sorted descending)
-            while (a < b) {
-              const int mid = (a + b) >> 1;
-              if (qb * Y.q[mid] < cut) b = mid;
-              else a = mid + 1;
-            }
-            hi = a;
-          }
-          if (x == y) hi = std::min(hi, bp + 1);
-          if (hi <= lo) continue;
-          W->quartets += hi - lo;
-          W->prim_quartets += npa * (Y.npp_prefix[hi] - Y.npp_prefix[lo]);
-          for (int s = lo; s < hi; s += chunk) items.push_back(make_int4(bp, s, std::min(hi, s + chunk), 0));
+      for_each_run(X, Y, x == y, [&](int bp, int lo, int hi) {
+        const long long npa = X.npp_pos[bp];
+        W->quartets += hi - lo;
+        W->prim_quartets += npa * (Y.npp_prefix[hi] - Y.npp_prefix[lo]);
+        for (int s = lo; s < hi; s += chunk) {
+          items.push_back(make_int4(bp, s, std::min(hi, s + chunk), 0));
+          W->item_cost.push_back(npa * (Y.npp_prefix[std::min(hi, s + chunk)] - Y.npp_prefix[s]));
         }
-      }
+      });
       W->nwork = (int)items.size();
       if (W->nwork == 0) { delete W; continue; }
       upload(W->work, items.data(), items.size() * sizeof(int4));
       W->h_items = items;
       W->all_items = items;
-      W->item_cost.resize(items.size());
-      for (size_t i = 0; i < items.size(); ++i) {
-        const int4 it = items[i];
-        W->item_cost[i] = (long long)p.pair_info[X.pairs[it.x]].w * (Y.npp_prefix[it.z] - Y.npp_prefix[it.y]);
-      }
       CUDA_OK(W->split.ensure(W->nwork * sizeof(int)));
+      // grouped lists for the J/K build where both precisions' kernels take them
+      W->grouped_x = disp.grouped[cls] && !p.grouped[x].q.empty();
+      W->grouped_y = disp.grouped[cls] && !p.grouped[y].q.empty();
+      if (W->grouped_x || W->grouped_y) {
+        const ClassList& GX = W->grouped_x ? p.grouped[x] : X;
+        const ClassList& GY = W->grouped_y ? p.grouped[y] : Y;
+        std::map<std::pair<int, int>, GenBucket*> by;
+        for_each_run(GX, GY, x == y, [&](int bp, int lo, int hi) {
+          const int gb = GX.nco.empty() ? 1 : GX.nco[bp];
+          const int gk = GY.nco.empty() ? 1 : GY.nco[lo];
+          GenBucket*& B = by[{gb, gk}];
+          if (!B) {
+            B = new GenBucket();
+            B->gb = gb;
+            B->gk = gk;
+          }
+          const long long npa = GX.npp_pos[bp];
+          B->quartets += (long long)(hi - lo) * gb * gk;
+          B->prim_quartets += npa * (GY.npp_prefix[hi] - GY.npp_prefix[lo]);
+          for (int s = lo; s < hi; s += 64) {
+            const int e = std::min(hi, s + 64);
+            B->all_items.push_back(make_int4(bp, s, e, 0));
+            B->item_cost.push_back(npa * (GY.npp_prefix[e] - GY.npp_prefix[s]) * (gb * gk > 1 ? 2 : 1));
+          }
+        });
+        for (auto& kv : by) {
+          GenBucket* B = kv.second;
+          B->h_items = B->all_items;
+          B->nwork = (int)B->all_items.size();
+          upload(B->work, B->all_items.data(), B->all_items.size() * sizeof(int4));
+          CUDA_OK(B->split.ensure(B->nwork * sizeof(int)));
+          W->buckets.push_back(B);
+        }
+      }
       p.work.push_back(W);
     }
   // ---- quartet count on the reference's shells (parent pairs, canonical)
@@ -840,13 +1132,14 @@ void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j,
     CUDA_OK(cudaMemsetAsync(p.d_maxd.ptr, 0, sizeof(double), st));
     maxabs_kernel<<<592, 256, 0, st>>>(d_in, (long long)nb * p.out_stride, p.d_maxd.as<double>());
     CUDA_OK(cudaGetLastError());
-    for (auto* W : p.work) {
-      if (W->nwork == 0) continue;  // nothing of this class pair on this shard
-      split_kernel<<<(W->nwork + 127) / 128, 128, 0, st>>>(
-          W->work.as<int4>(), p.classes[W->x].d_q.as<double>(), p.classes[W->y].d_q.as<double>(),
-          p.d_maxd.as<double>(), fp32_cut, W->nwork, W->split.as<int>());
-      CUDA_OK(cudaGetLastError());
-    }
+    for (auto* W : p.work)
+      for_each_unit(p, *W, [&](const JKUnit& u) {
+        if (u.nwork == 0) return;  // nothing of this class pair on this shard
+        split_kernel<<<(u.nwork + 127) / 128, 128, 0, st>>>(
+            u.work->as<int4>(), u.X->d_q.as<double>(), u.Y->d_q.as<double>(), p.d_maxd.as<double>(),
+            fp32_cut, u.nwork, u.split->as<int>());
+        CUDA_OK(cudaGetLastError());
+      });
   }
   JKArgs a = base_args(p);
   a.dens = s_dens;
@@ -860,33 +1153,39 @@ void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j,
   a.with_k = with_k;
   const auto& disp = dispatch();
   for (auto* W : p.work) {
-    if (W->nwork == 0) continue;
     const int cls = quartet_class(W->x, W->y);
-    set_lists(a, p, *W);
-    a.work = W->work.as<int4>();
-    a.nwork = W->nwork;
-    a.split = W->split.as<int>();
-    auto launch = [&](int mode, bool fp32) {
-      a.split_mode = mode;
-      ProfileEvent ev{cls, fp32 ? 1 : 0, nullptr, nullptr};
-      if (p.profiling && allow_profiling) {
-        CUDA_OK(cudaEventCreate(&ev.start));
-        CUDA_OK(cudaEventCreate(&ev.stop));
-        CUDA_OK(cudaEventRecord(ev.start, st));
+    for_each_unit(p, *W, [&](const JKUnit& u) {
+      if (u.nwork == 0) return;
+      set_unit_lists(a, u, W->x == W->y);
+      a.work = u.work->as<int4>();
+      a.nwork = u.nwork;
+      a.split = u.split->as<int>();
+      const bool plain = u.gb == 1 && u.gk == 1;
+      const JKLauncher l64 = plain ? disp.jk64[cls] : disp.jkg64[cls][gen_slot(u.gb, u.gk)];
+      const JKLauncher l32 = plain ? disp.jk32[cls] : disp.jkg32[cls][gen_slot(u.gb, u.gk)];
+      if (!l64 || !l32) throw Failure{B200JK_INTERNAL, "no kernel for this contraction grouping"};
+      auto launch = [&](int mode, bool fp32) {
+        a.split_mode = mode;
+        ProfileEvent ev{cls, fp32 ? 1 : 0, nullptr, nullptr};
+        if (p.profiling && allow_profiling) {
+          CUDA_OK(cudaEventCreate(&ev.start));
+          CUDA_OK(cudaEventCreate(&ev.stop));
+          CUDA_OK(cudaEventRecord(ev.start, st));
+        }
+        const int rc = fp32 ? l32(a, st) : l64(a, st);
+        if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+        if (p.profiling && allow_profiling) {
+          CUDA_OK(cudaEventRecord(ev.stop, st));
+          p.events.push_back(ev);
+        }
+      };
+      if (precision == B200JK_FP64) {
+        launch(0, false);
+      } else {
+        launch(1, false);
+        launch(2, true);
       }
-      const int rc = fp32 ? disp.jk32[cls](a, st) : disp.jk64[cls](a, st);
-      if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
-      if (p.profiling && allow_profiling) {
-        CUDA_OK(cudaEventRecord(ev.stop, st));
-        p.events.push_back(ev);
-      }
-    };
-    if (precision == B200JK_FP64) {
-      launch(0, false);
-    } else {
-      launch(1, false);
-      launch(2, true);
-    }
+    });
   }
   {
     const int no = max_no(p);
@@ -1111,26 +1410,32 @@ int b200jk_plan_set_shard(b200jk_plan* plan, int32_t rank, int32_t world) {
     Plan& p = *plan->p;
     CUDA_OK(cudaSetDevice(p.device));
     CUDA_OK(cudaDeviceSynchronize());
-    for (auto* W : p.work) {
-      const int64_t n = (int64_t)W->all_items.size();
+    // one partition per item list: the expanded items (coordinate VJP, and
+    // the J/K build of ungrouped class pairs) and every grouped bucket
+    auto shard = [&](const std::vector<int4>& all, const std::vector<int64_t>& cost, DevBuf& work,
+                     std::vector<int4>& h, int& nwork, long long& q, long long& pq, long long qmul) {
+      const int64_t n = (int64_t)all.size();
       std::vector<int32_t> owner(n);
-      if (b200jk_partition_items(W->item_cost.data(), n, world, owner.data()) != 0)
+      if (b200jk_partition_items(cost.data(), n, world, owner.data()) != 0)
         throw Failure{B200JK_INTERNAL, "work-item partition failed"};
       std::vector<int4> mine;
-      long long q = 0, pq = 0;
+      q = pq = 0;
       for (int64_t i = 0; i < n; ++i) {
         if (owner[i] != rank) continue;
-        const int4 it = W->all_items[i];
-        mine.push_back(it);
-        q += it.z - it.y;
-        pq += W->item_cost[i];
+        mine.push_back(all[i]);
+        q += (long long)(all[i].z - all[i].y) * qmul;
+        pq += cost[i];
       }
-      W->h_items = mine;
-      W->nwork = (int)mine.size();
-      W->quartets = q;
-      W->prim_quartets = pq;
+      h = mine;
+      nwork = (int)mine.size();
       if (!mine.empty())  // the buffer holds the full list, so it is never reallocated
-        CUDA_OK(cudaMemcpy(W->work.ptr, mine.data(), mine.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        CUDA_OK(cudaMemcpy(work.ptr, mine.data(), mine.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    };
+    for (auto* W : p.work) {
+      shard(W->all_items, W->item_cost, W->work, W->h_items, W->nwork, W->quartets, W->prim_quartets, 1);
+      for (auto* B : W->buckets)
+        shard(B->all_items, B->item_cost, B->work, B->h_items, B->nwork, B->quartets, B->prim_quartets,
+              (long long)B->gb * B->gk);
     }
     p.shard_rank = rank;
     p.shard_world = world;
@@ -1144,8 +1449,14 @@ int b200jk_plan_class_stats(const b200jk_plan* plan, int64_t* quartets, int64_t*
     std::fill(prim_quartets, prim_quartets + kQuartetClasses, 0);
     for (auto* W : plan->p->work) {
       const int c = quartet_class(W->x, W->y);
-      quartets[c] += W->quartets;
-      prim_quartets[c] += W->prim_quartets;
+      if (W->buckets.empty()) {
+        quartets[c] += W->quartets;
+        prim_quartets[c] += W->prim_quartets;
+      }
+      for (auto* B : W->buckets) {  // grouped: digested quartets, primitive quartets evaluated
+        quartets[c] += B->quartets;
+        prim_quartets[c] += B->prim_quartets;
+      }
     }
   });
 }
@@ -1160,19 +1471,23 @@ int b200jk_plan_split_stats(b200jk_plan* plan, void* stream, int64_t* q64, int64
     for (int c = 0; c < kQuartetClasses; ++c) q64[c] = q32[c] = pq64[c] = pq32[c] = 0;
     for (auto* W : p.work) {
       const int c = quartet_class(W->x, W->y);
-      std::vector<int> split(W->nwork);
-      CUDA_OK(cudaMemcpy(split.data(), W->split.ptr, W->nwork * sizeof(int), cudaMemcpyDeviceToHost));
-      const auto& pre = p.classes[W->y].npp_prefix;
-      for (int i = 0; i < W->nwork; ++i) {
-        const int4 it = W->h_items[i];
-        const int lo = it.y, hi = it.z;
-        const int sp = std::min(std::max(split[i], lo), hi);
-        const long long npa = p.pair_info[p.classes[W->x].pairs[it.x]].w;
-        q64[c] += sp - lo;
-        q32[c] += hi - sp;
-        pq64[c] += npa * (pre[sp] - pre[lo]);
-        pq32[c] += npa * (pre[hi] - pre[sp]);
-      }
+      for_each_unit(p, *W, [&](const JKUnit& u) {
+        if (u.nwork == 0) return;
+        std::vector<int> split(u.nwork);
+        CUDA_OK(cudaMemcpy(split.data(), u.split->ptr, u.nwork * sizeof(int), cudaMemcpyDeviceToHost));
+        const auto& pre = u.Y->npp_prefix;
+        const long long combos = (long long)u.gb * u.gk;
+        for (int i = 0; i < u.nwork; ++i) {
+          const int4 it = (*u.h_items)[i];
+          const int lo = it.y, hi = it.z;
+          const int sp = std::min(std::max(split[i], lo), hi);
+          const long long npa = u.X->npp_pos[it.x];
+          q64[c] += (sp - lo) * combos;
+          q32[c] += (hi - sp) * combos;
+          pq64[c] += npa * (pre[sp] - pre[lo]);
+          pq32[c] += npa * (pre[hi] - pre[sp]);
+        }
+      });
     }
   });
 }

@@ -72,6 +72,14 @@ int launch_class(const JKArgs& args, cudaStream_t stream) {
   return (int)cudaGetLastError();
 }
 
+template <int LA, int LB, int LC, int LD, typename R, int GB, int GK>
+int launch_gen(const JKArgs& args, cudaStream_t stream) {
+  if (args.nwork <= 0) return 0;
+  jk_reg_gen_kernel<LA, LB, LC, LD, R, GB, GK>
+      <<<(args.nwork + kRegWarps - 1) / kRegWarps, 32 * kRegWarps, 0, stream>>>(args);
+  return (int)cudaGetLastError();
+}
+
 #if BRA_CLASS == KET_CLASS
 template <int LA, int LB>
 int launch_schwarz(const JKArgs& args, int npairs, int cart, cudaStream_t stream) {
@@ -124,6 +132,22 @@ static_assert(Y <= X, "ket class must not exceed bra class");
 constexpr int XA = pc_la(X), XB = pc_lb(X);
 constexpr int YA = pc_la(Y), YB = pc_lb(Y);
 
+// Grouped lists: both precisions on the register path and an (l, 0) side;
+// up to 4 combinations on a (0, 0) pair, 2 on other (l, 0) pairs.
+constexpr bool GROUPED = Policy<XA, XB, YA, YB, float>::REG && Policy<XA, XB, YA, YB>::REG && (XB == 0 || YB == 0);
+
+constexpr int gslot(int g) { return g == 1 ? 0 : (g == 2 ? 1 : 2); }
+
+template <int GB, int GK>
+void register_gen(DispatchTable& t, int id) {
+  constexpr bool okb = GB == 1 || (XB == 0 && (GB == 2 || X == 0));
+  constexpr bool okk = GK == 1 || (YB == 0 && (GK == 2 || Y == 0));
+  if constexpr (GROUPED && okb && okk && !(GB == 1 && GK == 1)) {
+    t.jkg64[id][3 * gslot(GB) + gslot(GK)] = &launch_gen<XA, XB, YA, YB, double, GB, GK>;
+    t.jkg32[id][3 * gslot(GB) + gslot(GK)] = &launch_gen<XA, XB, YA, YB, float, GB, GK>;
+  }
+}
+
 }  // namespace
 
 #define CAT4(a, b, c, d) a##b##c##d
@@ -135,6 +159,15 @@ void REG_NAME(BRA_CLASS, KET_CLASS)(DispatchTable& t) {
   t.grad64[id] = &launch_grad<XA, XB, YA, YB>;
   t.reg_path[id] = Policy<XA, XB, YA, YB, float>::REG || Policy<XA, XB, YA, YB>::REG;
   t.tile[id] = Policy<XA, XB, YA, YB>::TILE;
+  t.grouped[id] = GROUPED;
+  register_gen<1, 2>(t, id);
+  register_gen<1, 4>(t, id);
+  register_gen<2, 1>(t, id);
+  register_gen<2, 2>(t, id);
+  register_gen<2, 4>(t, id);
+  register_gen<4, 1>(t, id);
+  register_gen<4, 2>(t, id);
+  register_gen<4, 4>(t, id);
   t.team[id] = Policy<XA, XB, YA, YB>::REG ? 1
                : (Policy<XA, XB, YA, YB>::TILE ? TileCfg<XA, XB, YA, YB, double>::THREADS / 4
                                                : Policy<XA, XB, YA, YB>::TEAM);

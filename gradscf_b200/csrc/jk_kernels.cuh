@@ -36,6 +36,10 @@ struct JKArgs {
   // pair, count, Cartesian offset of A, of B); same_list: bra list == ket list
   const double4 *bra_ra, *bra_ab, *ket_ra, *ket_ab;
   const int4 *bra_ix, *ket_ix;
+  // grouped lists: (diag, 0, aoA1, aoB1), (aoA2, aoB2, aoA3, aoB3) per position
+  const int4 *bra_gx, *bra_gy, *ket_gx, *ket_gy;
+  const double4* pp_c;       // per primitive pair: coefficients of up to 4 combinations
+  const float4* pp_cf;       // the same in FP32
   int same_list;
   const int4* work;          // (bra position, ket begin, ket end, unused)
   int nwork;
@@ -500,12 +504,12 @@ __device__ __forceinline__ void digest_reg(const JKArgs& args, const QuartetGeom
 }
 
 // Occupancy target of the register path from its estimated register need.
-template <int LA, int LB, int LC, int LD, typename R>
+template <int LA, int LB, int LC, int LD, typename R, int NACC = ClassInfo<LA, LB, LC, LD>::NOUT>
 struct RegMinBlocks {
   using CI = ClassInfo<LA, LB, LC, LD>;
-  // estimated live registers: output block + one root's 2D integrals + ~70 for
+  // estimated live registers: accumulators + one root's 2D integrals + ~70 for
   // addresses, primitive scalars and digestion (FP64 values take two)
-  static constexpr int EST = (sizeof(R) == 8 ? 2 : 1) * (CI::NOUT + 3 * CI::NG) + 70;
+  static constexpr int EST = (sizeof(R) == 8 ? 2 : 1) * (NACC + 3 * CI::NG) + 70;
   static constexpr int base = EST <= 84 ? 6 : (EST <= 100 ? 5 : (EST <= 124 ? 4 : (EST <= 160 ? 3 : 2)));
 #ifndef B200JK_MINB_DELTA
 #define B200JK_MINB_DELTA 0
@@ -586,6 +590,215 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
       const double v = s_jab[warp][ab];
       if (v != 0.0) atomicAdd(vj + (long long)(br.ix.z + ab / CI::NB) * n + br.ix.w + ab % CI::NB, v);
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Register path on grouped lists: a bra entry carries GB contraction
+// combinations of its parent shell pair and a ket entry GK; the primitive
+// pairs are shared by the combinations and carry their coefficients
+// (pp_c), so each primitive quartet is evaluated once and added, weighted,
+// to the GB*GK contracted blocks.  Every combination is digested like a
+// quartet of work shells; a diagonal parent pair (A and B the same shell)
+// holds both orders of its combinations, each digested with weight 1/2.
+// ---------------------------------------------------------------------------
+template <typename R> struct CoefSel;
+template <> struct CoefSel<double> {
+  using T = double4;
+  static __device__ __forceinline__ T get(const JKArgs& a, int i) { return a.pp_c[i]; }
+};
+template <> struct CoefSel<float> {
+  using T = float4;
+  static __device__ __forceinline__ T get(const JKArgs& a, int i) { return a.pp_cf[i]; }
+};
+template <int K, typename C4>
+__device__ __forceinline__ auto comp(const C4& v) {
+  if constexpr (K == 0) return v.x;
+  else if constexpr (K == 1) return v.y;
+  else if constexpr (K == 2) return v.z;
+  else return v.w;
+}
+
+template <int LA, int LB, int LC, int LD, typename R, int GB, int GK>
+__device__ __forceinline__ void quartet_block_gen(const JKArgs& args, const QuartetGeom& g,
+                                                  const typename PrimData<R>::A* bpp,
+                                                  const typename PrimData<R>::B* baux,
+                                                  const typename CoefSel<R>::T* bco, R* out,
+                                                  const float* s_boys) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using GI = GIdx<LA, LB, LC, LD>;
+  constexpr int N = CI::NROOT, NO = CI::NOUT;
+#pragma unroll
+  for (int o = 0; o < GB * GK * NO; ++o) out[o] = R(0);
+  const float3 ac = make_float3(float(g.ax - g.cx), float(g.ay - g.cy), float(g.az - g.cz));
+  auto Qn = PrimData<R>::a(args, g.ppc);
+  auto QAn = PrimData<R>::b(args, g.ppc);
+  auto Cn = CoefSel<R>::get(args, g.ppc);
+  for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
+    const auto Q = Qn;
+    const auto QA = QAn;
+    const auto CK = Cn;
+    if (j + 1 < g.ppc + g.npc) {
+      Qn = PrimData<R>::a(args, j + 1);
+      QAn = PrimData<R>::b(args, j + 1);
+      Cn = CoefSel<R>::get(args, j + 1);
+    }
+    for (int i = 0; i < g.npa; ++i) {
+      PrimQ<R> s;
+      prim_any<R>(g, ac, bpp[i], baux[i], Q, QA, s);
+      R x[N], w[N];
+      if constexpr (sizeof(R) == 4 && N <= 3)
+        rys_small<N, float, 10, 6>(s.t, x, w, s_boys);
+      else
+        rys_roots<N, R>(s.t, x, w, args.tb);
+      R tmp[NO];
+#pragma unroll
+      for (int o = 0; o < NO; ++o) tmp[o] = R(0);
+#pragma unroll
+      for (int r = 0; r < N; ++r) {
+        RootCoef<R> rc;
+        root_coef<R>(s, x[r], rc);
+        R gx[CI::NG], gy[CI::NG], gz[CI::NG];
+        build_g<LA, LB, LC, LD, R>(rc.c00[0], rc.c0p[0], rc.b10, rc.b01, rc.b00, R(1), R(g.abx),
+                                   R(g.cdx), gx);
+        build_g<LA, LB, LC, LD, R>(rc.c00[1], rc.c0p[1], rc.b10, rc.b01, rc.b00, R(1), R(g.aby),
+                                   R(g.cdy), gy);
+        build_g<LA, LB, LC, LD, R>(rc.c00[2], rc.c0p[2], rc.b10, rc.b01, rc.b00, w[r] * s.pref,
+                                   R(g.abz), R(g.cdz), gz);
+        static_for<0, NO>([&](auto O) {
+          constexpr int o = decltype(O)::value;
+          constexpr int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
+          constexpr int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
+          constexpr int jx = GI::idx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
+          constexpr int jy = GI::idx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
+          constexpr int jz = GI::idx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
+          tmp[o] += gx[jx] * gy[jy] * gz[jz];
+        });
+      }
+      const auto CB = bco[i];
+      static_for<0, GB>([&](auto BI) {
+        constexpr int b = decltype(BI)::value;
+        const R cb = R(comp<b>(CB));
+        static_for<0, GK>([&](auto KI) {
+          constexpr int k = decltype(KI)::value;
+          const R wgt = cb * R(comp<k>(CK));
+#pragma unroll
+          for (int o = 0; o < NO; ++o) out[(b * GK + k) * NO + o] += wgt * tmp[o];
+        });
+      });
+    }
+  }
+}
+
+template <int LA, int LB, int LC, int LD, typename R, int GB, int GK>
+__global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
+                                                     (GB * GK + 1) * ClassInfo<LA, LB, LC, LD>::NOUT>::value))
+    jk_reg_gen_kernel(JKArgs args) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using PA_t = typename PrimData<R>::A;
+  using PB_t = typename PrimData<R>::B;
+  using C4 = typename CoefSel<R>::T;
+  constexpr int NO = CI::NOUT;
+  __shared__ PA_t s_pp[kRegWarps][kBraPrimCache];
+  __shared__ PB_t s_aux[kRegWarps][kBraPrimCache];
+  __shared__ C4 s_co[kRegWarps][kBraPrimCache];
+  __shared__ double s_jab[kRegWarps][GB * CI::NAB];
+  constexpr bool kSharedBoys = sizeof(R) == 4 && CI::NROOT <= 3;
+  __shared__ __align__(16) float s_boys[kSharedBoys ? 401 * 8 : 4];
+  if constexpr (kSharedBoys) {
+    const float4* src = reinterpret_cast<const float4*>(args.tb.boys_s_f + (CI::NROOT - 1) * 401 * 8);
+    float4* dst = reinterpret_cast<float4*>(s_boys);
+    for (int i = threadIdx.x; i < 401 * 2; i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.x * kRegWarps + warp;
+  if (item >= args.nwork) return;
+  const int4 w = args.work[item];
+  int kb = w.y, ke = w.z;
+  if (args.split_mode != 0) {
+    const int sp = args.split[item];
+    if (args.split_mode == 1) ke = min(ke, sp);
+    else kb = max(kb, sp);
+  }
+  if (kb >= ke) return;
+  const BraRec br = load_bra(args, w.x);
+  const int ppb = br.ix.x, npb = br.ix.y;
+  // bra combinations: Cartesian offsets of A and B, parent-diagonal flag
+  int aoA[GB], aoB[GB];
+  bool bdiag;
+  {
+    int4 gx = make_int4(br.ix.z == br.ix.w, 0, 0, 0), gy = make_int4(0, 0, 0, 0);
+    if constexpr (GB > 1) {
+      gx = args.bra_gx[w.x];
+      gy = args.bra_gy[w.x];
+    }
+    const int a4[4] = {br.ix.z, gx.z, gy.x, gy.z}, b4[4] = {br.ix.w, gx.w, gy.y, gy.w};
+#pragma unroll
+    for (int b = 0; b < GB; ++b) { aoA[b] = a4[b]; aoB[b] = b4[b]; }
+    bdiag = gx.x != 0;
+  }
+  const bool cached = npb <= kBraPrimCache;
+  if (cached)
+    for (int i = lane; i < npb; i += 32) {
+      s_pp[warp][i] = PrimData<R>::a(args, ppb + i);
+      s_aux[warp][i] = PrimData<R>::b(args, ppb + i);
+      s_co[warp][i] = CoefSel<R>::get(args, ppb + i);
+    }
+  const bool acc_j = args.with_j && args.nsym == 1;
+  for (int i = lane; i < GB * CI::NAB; i += 32) s_jab[warp][i] = 0.0;
+  __syncwarp();
+  const PA_t* bpp = cached ? s_pp[warp] : (sizeof(R) == 4 ? (const PA_t*)(args.pp_f + ppb)
+                                                         : (const PA_t*)(args.pp_data + ppb));
+  const PB_t* baux = cached ? s_aux[warp] : (sizeof(R) == 4 ? (const PB_t*)(args.pp_f2 + ppb)
+                                                           : (const PB_t*)(args.pp_aux + ppb));
+  const C4* bco = cached ? s_co[warp] : (sizeof(R) == 4 ? (const C4*)(args.pp_cf + ppb)
+                                                       : (const C4*)(args.pp_c + ppb));
+  QuartetGeom g;
+  for (int k0 = kb; k0 < ke; k0 += 32) {
+    const bool active = k0 + lane < ke;
+    const int k = active ? k0 + lane : ke - 1;
+    load_quartet_rec(args, br, k, g);
+    int aoC[GK], aoD[GK];
+    bool kdiag;
+    {
+      int4 gx = make_int4(g.aoC == g.aoD, 0, 0, 0), gy = make_int4(0, 0, 0, 0);
+      if constexpr (GK > 1) {
+        gx = args.ket_gx[k];
+        gy = args.ket_gy[k];
+      }
+      const int c4[4] = {g.aoC, gx.z, gy.x, gy.z}, d4[4] = {g.aoD, gx.w, gy.y, gy.w};
+#pragma unroll
+      for (int c = 0; c < GK; ++c) { aoC[c] = c4[c]; aoD[c] = d4[c]; }
+      kdiag = gx.x != 0;
+    }
+    const double sbk = (bdiag ? 0.5 : 1.0) * (kdiag ? 0.5 : 1.0) * (args.same_list && k == w.x ? 0.5 : 1.0);
+    R out[GB * GK * NO];
+    quartet_block_gen<LA, LB, LC, LD, R, GB, GK>(args, g, bpp, baux, bco, out, s_boys);
+#pragma unroll
+    for (int b = 0; b < GB; ++b)
+#pragma unroll
+      for (int c = 0; c < GK; ++c) {
+        QuartetGeom gc = g;
+        gc.aoA = aoA[b]; gc.aoB = aoB[b]; gc.aoC = aoC[c]; gc.aoD = aoD[c];
+        gc.scale = sbk;
+        DensPre<LA, LB, LC, LD, R> pre;
+        pre.load(args, gc);
+        digest_reg<LA, LB, LC, LD, R>(args, gc, out + (b * GK + c) * NO, acc_j, active,
+                                      s_jab[warp] + b * CI::NAB, pre);
+      }
+  }
+  if (acc_j) {
+    __syncwarp();
+    const int mol = (int)br.ra.w;
+    double* vj = args.vj + args.mol_base[mol];
+    const int n = args.mol_n[mol];
+#pragma unroll
+    for (int b = 0; b < GB; ++b)
+      for (int ab = lane; ab < CI::NAB; ab += 32) {
+        const double v = s_jab[warp][b * CI::NAB + ab];
+        if (v != 0.0) atomicAdd(vj + (long long)(aoA[b] + ab / CI::NB) * n + aoB[b] + ab % CI::NB, v);
+      }
   }
 }
 

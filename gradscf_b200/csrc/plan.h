@@ -33,6 +33,17 @@ struct DevBuf {
   template <typename T> T* as() const { return static_cast<T*>(ptr); }
 };
 
+// Work items of a class pair on grouped lists whose bra / ket entries carry
+// gb / gk contraction combinations (one kernel instantiation per bucket).
+struct GenBucket {
+  int gb = 1, gk = 1;
+  int nwork = 0;
+  DevBuf work, split;
+  std::vector<int4> h_items, all_items;
+  std::vector<int64_t> item_cost;
+  long long quartets = 0, prim_quartets = 0;
+};
+
 struct ClassPairWork {
   int x = 0, y = 0;             // bra / ket pair classes
   int nwork = 0;
@@ -44,6 +55,13 @@ struct ClassPairWork {
   std::vector<int4> h_items;    // host copy of the active work items (this rank's shard)
   std::vector<int4> all_items;  // every work item of the class pair
   std::vector<int64_t> item_cost;  // primitive quartets per item (all_items order)
+  // grouped lists (contraction combinations shared): the J/K work is in
+  // `buckets`; `work` still holds the expanded items (coordinate VJP)
+  bool grouped_x = false, grouped_y = false;
+  std::vector<GenBucket*> buckets;
+  ~ClassPairWork() {
+    for (auto* b : buckets) delete b;
+  }
 };
 
 struct ClassList {
@@ -52,11 +70,17 @@ struct ClassList {
   std::vector<int> mol_begin;   // per molecule: first position (size nmol+1)
   std::vector<std::vector<int2>> segs;  // per molecule: [begin, end) runs of equal primitive-pair count
   std::vector<long long> npp_prefix;  // prefix sums of primitive-pair counts (size+1)
+  std::vector<int> npp_pos, mol_pos;  // per position: primitive pairs, molecule
   DevBuf d_pairs, d_q;
   // per list position (coalesced reads by consecutive kets): centre A and
   // molecule (Ax, Ay, Az, mol), A - B, and (first primitive pair, count,
   // Cartesian offset of A, of B) in the molecule
   DevBuf d_ra, d_ab, d_ix;
+  // grouped lists only: contraction combinations per entry (1, 2 or 4) and,
+  // per position, (diag, 0, aoA1, aoB1) and (aoA2, aoB2, aoA3, aoB3); segs
+  // are then runs of equal (combinations, primitive-pair count)
+  std::vector<int> nco;
+  DevBuf d_gx, d_gy;
 };
 
 struct ProfileEvent {
@@ -91,11 +115,13 @@ struct Plan {
   std::vector<int> pair_class;
   std::vector<double> pair_q;    // parent Schwarz bound
   ClassList classes[kPairClasses];
+  ClassList grouped[kPairClasses];  // pair classes (l, 0) only: parent pairs with combinations
   std::vector<ClassPairWork*> work;
   long long quartets = 0;
   // nuclei (for one-electron terms): global atm rows with charge
   std::vector<double4> atom_xyzq; // (x, y, z, charge) per global atm row
   // device tables
+  DevBuf d_pp_c, d_pp_cf;          // per primitive pair: combination coefficients (FP64, FP32)
   DevBuf d_ws_info, d_ws_xyz, d_pair_info, d_pp_data, d_pp_aux, d_pp_exp, d_pp_f, d_pp_f2, d_mol_base_cart, d_mol_ncart,
       d_mol_base_out, d_mol_nout, d_cart_ws, d_out_ws, d_status, d_maxd, d_q_work, d_atoms,
       d_ws_atm, d_mol_ao_off, d_ws_prim, d_ws_prim_off;
