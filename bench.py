@@ -201,6 +201,13 @@ def main():
     quartets = plan.quartets
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
+    # autotune the register-path tile shape (kets per work item) on a
+    # representative incremental dD: the last warm-up iteration's (untimed)
+    tune_delta = []
+    scf.rhf(mol, precision="split", fp32_cut=FP32_CUT, fixed_cycles=args.warmup + 1, density0=d0,
+            on_jk=lambda c, dd: tune_delta.append(dd.clone()) if c == args.warmup + 1 else None)
+    tuned = plan.autotune(tune_delta[0].reshape(1, -1), hermi=1, precision="split", fp32_cut=FP32_CUT)
+
     peaks = {}
     for name, flag in (("fp64", 1), ("fp32", 0)):
         v = ctypes.c_double()
@@ -343,6 +350,7 @@ def main():
                        "scf": f"fragment guess (converged monomer densities), DIIS(8), {W} untimed + {K} timed iterations per mode",
                        "quartets_per_build": quartets, "nao": n, "fp32_cut": FP32_CUT,
                        "l2": "flushed (512 MB write) before every timed build",
+                       "autotuned_kets_per_item": tuned,
                        "parallelism": f"J/K work-item shards x{world} + NCCL all-reduce" if world > 1 else "single GPU"},
             "s_per_iter": {"split": results["split"]["ms"] * 1e-3, "fp64": results["fp64"]["ms"] * 1e-3},
             "fp64": fp64_build,

@@ -481,6 +481,153 @@ static JKArgs base_args(const Plan& p) {
   return a;
 }
 
+// (bra position, ket run [lo, hi)) of every bra: the Schwarz-screened
+// prefix of each ket run of the bra's molecule, canonical when X == Y
+template <typename F>
+static void for_each_run(const ClassList& X, const ClassList& Y, bool same, double cut, F&& emit) {
+  for (int bp = 0; bp < (int)X.q.size(); ++bp) {
+    const int m = X.mol_pos[bp];
+    const double qb = X.q[bp];
+    for (const int2 seg : Y.segs[m]) {
+      const int lo = seg.x;
+      if (same && lo > bp) break;  // canonical: ket position <= bra position
+      int hi = seg.y;
+      if (cut > 0) {
+        int a = lo, b = seg.y;  // first ket with qb*qk < cut (bounds sorted descending)
+        while (a < b) {
+          const int mid = (a + b) >> 1;
+          if (qb * Y.q[mid] < cut) b = mid;
+          else a = mid + 1;
+        }
+        hi = a;
+      }
+      if (same) hi = std::min(hi, bp + 1);
+      if (hi > lo) emit(bp, lo, hi);
+    }
+  }
+}
+
+#ifndef B200JK_TILE_CHUNK
+#define B200JK_TILE_CHUNK 64   // kets per tile-path work item (measured best of 16/32/64)
+#endif
+#ifndef B200JK_REG_CHUNK
+#define B200JK_REG_CHUNK 64    // kets per register-path work item (two 32-ket passes of a warp)
+#endif
+#ifndef B200JK_HEAVY_PQ
+#define B200JK_HEAVY_PQ 64  // primitive quartets per quartet from which items take 32 kets (measured)
+#endif
+
+// register path: items of heavy quartets (many primitive pairs on both
+// sides) take one 32-ket pass, so long items do not form the launch's tail
+static int reg_chunk(long long npa, long long npc) {
+  return npa * npc >= (long long)(B200JK_HEAVY_PQ) ? 32 : B200JK_REG_CHUNK;
+}
+
+static void upload_items(DevBuf& work, DevBuf& split, const std::vector<int4>& items) {
+  CUDA_OK(work.ensure(std::max<size_t>(items.size(), 1) * sizeof(int4)));
+  if (!items.empty())
+    CUDA_OK(cudaMemcpy(work.ptr, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  CUDA_OK(split.ensure(std::max<size_t>(items.size(), 1) * sizeof(int)));
+}
+
+// (Re)build the work items of class pair W: the expanded items and, where
+// both precisions' kernels take grouped lists, the grouped buckets.
+// `force` > 0 sets the ket chunk of the items the J/K build launches on the
+// register path (the autotuner's knob); 0 keeps the default rule.
+static void fill_items(Plan& p, ClassPairWork& W, int force) {
+  const auto& disp = dispatch();
+  const int x = W.x, y = W.y;
+  const ClassList& X = p.classes[x];
+  const ClassList& Y = p.classes[y];
+  const int cls = quartet_class(x, y);
+  const double cut = p.cutoff;
+  W.grouped_x = disp.grouped[cls] && !p.grouped[x].q.empty();
+  W.grouped_y = disp.grouped[cls] && !p.grouped[y].q.empty();
+  const bool grouped = W.grouped_x || W.grouped_y;
+  const int chunk0 = disp.reg_path[cls] ? B200JK_REG_CHUNK : std::max(8, 4 * (128 / disp.team[cls]));
+  std::vector<int4> items;
+  W.quartets = W.prim_quartets = 0;
+  W.item_cost.clear();
+  for_each_run(X, Y, x == y, cut, [&](int bp, int lo, int hi) {
+    const long long npa = X.npp_pos[bp];
+    int chunk = chunk0;
+    if (disp.tile[cls] && B200JK_TILE_CHUNK > 0) chunk = B200JK_TILE_CHUNK;
+    else if (disp.reg_path[cls]) chunk = (force > 0 && !grouped) ? force : reg_chunk(npa, Y.npp_pos[lo]);
+    W.quartets += hi - lo;
+    W.prim_quartets += npa * (Y.npp_prefix[hi] - Y.npp_prefix[lo]);
+    for (int s = lo; s < hi; s += chunk) {
+      const int e = std::min(hi, s + chunk);
+      items.push_back(make_int4(bp, s, e, 0));
+      W.item_cost.push_back(npa * (Y.npp_prefix[e] - Y.npp_prefix[s]));
+    }
+  });
+  W.nwork = (int)items.size();
+  upload_items(W.work, W.split, items);
+  W.h_items = items;
+  W.all_items = items;
+  for (auto* B : W.buckets) delete B;
+  W.buckets.clear();
+  if (!grouped) return;
+  const ClassList& GX = W.grouped_x ? p.grouped[x] : X;
+  const ClassList& GY = W.grouped_y ? p.grouped[y] : Y;
+  std::map<std::pair<int, int>, GenBucket*> by;
+  for_each_run(GX, GY, x == y, cut, [&](int bp, int lo, int hi) {
+    const int gb = GX.nco.empty() ? 1 : GX.nco[bp];
+    const int gk = GY.nco.empty() ? 1 : GY.nco[lo];
+    GenBucket*& B = by[{gb, gk}];
+    if (!B) {
+      B = new GenBucket();
+      B->gb = gb;
+      B->gk = gk;
+    }
+    const long long npa = GX.npp_pos[bp];
+    B->quartets += (long long)(hi - lo) * gb * gk;
+    B->prim_quartets += npa * (GY.npp_prefix[hi] - GY.npp_prefix[lo]);
+    const int gchunk = force > 0 ? force : reg_chunk(npa, GY.npp_pos[lo]);
+    for (int s = lo; s < hi; s += gchunk) {
+      const int e = std::min(hi, s + gchunk);
+      B->all_items.push_back(make_int4(bp, s, e, 0));
+      B->item_cost.push_back(npa * (GY.npp_prefix[e] - GY.npp_prefix[s]) * (gb * gk > 1 ? 2 : 1));
+    }
+  });
+  for (auto& kv : by) {
+    GenBucket* B = kv.second;
+    B->h_items = B->all_items;
+    B->nwork = (int)B->all_items.size();
+    upload_items(B->work, B->split, B->all_items);
+    W.buckets.push_back(B);
+  }
+}
+
+// Restrict class pair W to the plan's shard: contiguous cost-balanced blocks
+// of every item list (expanded items and grouped buckets).
+static void apply_shard(Plan& p, ClassPairWork& W) {
+  const int rank = p.shard_rank, world = p.shard_world;
+  auto shard = [&](const std::vector<int4>& all, const std::vector<int64_t>& cost, DevBuf& work,
+                   std::vector<int4>& h, int& nwork, long long& q, long long& pq, long long qmul) {
+    const int64_t n = (int64_t)all.size();
+    std::vector<int32_t> owner(n);
+    if (b200jk_partition_items(cost.data(), n, world, owner.data()) != 0)
+      throw Failure{B200JK_INTERNAL, "work-item partition failed"};
+    std::vector<int4> mine;
+    q = pq = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      if (owner[i] != rank) continue;
+      mine.push_back(all[i]);
+      q += (long long)(all[i].z - all[i].y) * qmul;
+      pq += cost[i];
+    }
+    h = mine;
+    nwork = (int)mine.size();
+    if (!mine.empty())  // the buffer holds the full list, so it is never reallocated
+      CUDA_OK(cudaMemcpy(work.ptr, mine.data(), mine.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  };
+  shard(W.all_items, W.item_cost, W.work, W.h_items, W.nwork, W.quartets, W.prim_quartets, 1);
+  for (auto* B : W.buckets)
+    shard(B->all_items, B->item_cost, B->work, B->h_items, B->nwork, B->quartets, B->prim_quartets,
+          (long long)B->gb * B->gk);
+}
+
 // One entry of a grouped list (pair classes (l, 0)): a parent shell pair
 // with nco contraction combinations (work shells ws[k] on A, wsb[k] on B).
 struct GenEntry {
@@ -933,96 +1080,15 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     upload(L.d_gy, gy.data(), n * sizeof(int4));
   }
   // ---- work items per class pair (X >= Y)
-  const auto& disp = dispatch();
-  // (bra position, ket run [lo, hi)) of every bra: the Schwarz-screened
-  // prefix of each ket run of the bra's molecule, canonical when X == Y
-  auto for_each_run = [&](const ClassList& X, const ClassList& Y, bool same, auto&& emit) {
-    for (int bp = 0; bp < (int)X.q.size(); ++bp) {
-      const int m = X.mol_pos[bp];
-      const double qb = X.q[bp];
-      for (const int2 seg : Y.segs[m]) {
-        const int lo = seg.x;
-        if (same && lo > bp) break;  // canonical: ket position <= bra position
-        int hi = seg.y;
-        if (cut > 0) {
-          int a = lo, b = seg.y;  // first ket with qb*qk < cut (bounds sorted descending)
-          while (a < b) {
-            const int mid = (a + b) >> 1;
-            if (qb * Y.q[mid] < cut) b = mid;
-            else a = mid + 1;
-          }
-          hi = a;
-        }
-        if (same) hi = std::min(hi, bp + 1);
-        if (hi > lo) emit(bp, lo, hi);
-      }
-    }
-  };
-#ifndef B200JK_TILE_CHUNK
-#define B200JK_TILE_CHUNK 64   // kets per tile-path work item (measured best of 16/32/64)
-#endif
   for (int x = 0; x < kPairClasses; ++x)
     for (int y = 0; y <= x; ++y) {
-      const ClassList& X = p.classes[x];
-      const ClassList& Y = p.classes[y];
-      if (X.pairs.empty() || Y.pairs.empty()) continue;
-      const int cls = quartet_class(x, y);
-      int chunk = disp.reg_path[cls] ? 64 : std::max(8, 4 * (128 / disp.team[cls]));
-      if (B200JK_TILE_CHUNK > 0 && disp.tile[cls]) chunk = B200JK_TILE_CHUNK;
+      if (p.classes[x].pairs.empty() || p.classes[y].pairs.empty()) continue;
       auto* W = new ClassPairWork();
       W->x = x;
       W->y = y;
-      W->nbra = (int)X.pairs.size();
-      std::vector<int4> items;
-      for_each_run(X, Y, x == y, [&](int bp, int lo, int hi) {
-        const long long npa = X.npp_pos[bp];
-        W->quartets += hi - lo;
-        W->prim_quartets += npa * (Y.npp_prefix[hi] - Y.npp_prefix[lo]);
-        for (int s = lo; s < hi; s += chunk) {
-          items.push_back(make_int4(bp, s, std::min(hi, s + chunk), 0));
-          W->item_cost.push_back(npa * (Y.npp_prefix[std::min(hi, s + chunk)] - Y.npp_prefix[s]));
-        }
-      });
-      W->nwork = (int)items.size();
+      W->nbra = (int)p.classes[x].pairs.size();
+      fill_items(p, *W, 0);
       if (W->nwork == 0) { delete W; continue; }
-      upload(W->work, items.data(), items.size() * sizeof(int4));
-      W->h_items = items;
-      W->all_items = items;
-      CUDA_OK(W->split.ensure(W->nwork * sizeof(int)));
-      // grouped lists for the J/K build where both precisions' kernels take them
-      W->grouped_x = disp.grouped[cls] && !p.grouped[x].q.empty();
-      W->grouped_y = disp.grouped[cls] && !p.grouped[y].q.empty();
-      if (W->grouped_x || W->grouped_y) {
-        const ClassList& GX = W->grouped_x ? p.grouped[x] : X;
-        const ClassList& GY = W->grouped_y ? p.grouped[y] : Y;
-        std::map<std::pair<int, int>, GenBucket*> by;
-        for_each_run(GX, GY, x == y, [&](int bp, int lo, int hi) {
-          const int gb = GX.nco.empty() ? 1 : GX.nco[bp];
-          const int gk = GY.nco.empty() ? 1 : GY.nco[lo];
-          GenBucket*& B = by[{gb, gk}];
-          if (!B) {
-            B = new GenBucket();
-            B->gb = gb;
-            B->gk = gk;
-          }
-          const long long npa = GX.npp_pos[bp];
-          B->quartets += (long long)(hi - lo) * gb * gk;
-          B->prim_quartets += npa * (GY.npp_prefix[hi] - GY.npp_prefix[lo]);
-          for (int s = lo; s < hi; s += 64) {
-            const int e = std::min(hi, s + 64);
-            B->all_items.push_back(make_int4(bp, s, e, 0));
-            B->item_cost.push_back(npa * (GY.npp_prefix[e] - GY.npp_prefix[s]) * (gb * gk > 1 ? 2 : 1));
-          }
-        });
-        for (auto& kv : by) {
-          GenBucket* B = kv.second;
-          B->h_items = B->all_items;
-          B->nwork = (int)B->all_items.size();
-          upload(B->work, B->all_items.data(), B->all_items.size() * sizeof(int4));
-          CUDA_OK(B->split.ensure(B->nwork * sizeof(int)));
-          W->buckets.push_back(B);
-        }
-      }
       p.work.push_back(W);
     }
   // ---- quartet count on the reference's shells (parent pairs, canonical)
@@ -1102,6 +1168,57 @@ void check_jk_args(const Plan& p, const double* d_in, int nb, const double* d_ou
   if (!d_in || !d_out) invalid("Null density or output pointer");
 }
 
+// The FP32/FP64 boundary of every item of class pair W (split mode).
+static void split_units(Plan& p, ClassPairWork& W, double fp32_cut, cudaStream_t st) {
+  for_each_unit(p, W, [&](const JKUnit& u) {
+    if (u.nwork == 0) return;  // nothing of this class pair on this shard
+    split_kernel<<<(u.nwork + 127) / 128, 128, 0, st>>>(u.work->as<int4>(), u.X->d_q.as<double>(),
+                                                       u.Y->d_q.as<double>(), p.d_maxd.as<double>(),
+                                                       fp32_cut, u.nwork, u.split->as<int>());
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+// The J/K kernels of class pair W (both slices in split mode), on the
+// densities and accumulators already set in `a`.
+static void launch_units(Plan& p, ClassPairWork& W, JKArgs a, int precision, cudaStream_t st,
+                         bool allow_profiling) {
+  const auto& disp = dispatch();
+  const int cls = quartet_class(W.x, W.y);
+  for_each_unit(p, W, [&](const JKUnit& u) {
+    if (u.nwork == 0) return;
+    set_unit_lists(a, u, W.x == W.y);
+    a.work = u.work->as<int4>();
+    a.nwork = u.nwork;
+    a.split = u.split->as<int>();
+    const bool plain = u.gb == 1 && u.gk == 1;
+    const JKLauncher l64 = plain ? disp.jk64[cls] : disp.jkg64[cls][gen_slot(u.gb, u.gk)];
+    const JKLauncher l32 = plain ? disp.jk32[cls] : disp.jkg32[cls][gen_slot(u.gb, u.gk)];
+    if (!l64 || !l32) throw Failure{B200JK_INTERNAL, "no kernel for this contraction grouping"};
+    auto launch = [&](int mode, bool fp32) {
+      a.split_mode = mode;
+      ProfileEvent ev{cls, fp32 ? 1 : 0, nullptr, nullptr};
+      if (p.profiling && allow_profiling) {
+        CUDA_OK(cudaEventCreate(&ev.start));
+        CUDA_OK(cudaEventCreate(&ev.stop));
+        CUDA_OK(cudaEventRecord(ev.start, st));
+      }
+      const int rc = fp32 ? l32(a, st) : l64(a, st);
+      if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+      if (p.profiling && allow_profiling) {
+        CUDA_OK(cudaEventRecord(ev.stop, st));
+        p.events.push_back(ev);
+      }
+    };
+    if (precision == B200JK_FP64) {
+      launch(0, false);
+    } else {
+      launch(1, false);
+      launch(2, true);
+    }
+  });
+}
+
 // The J/K pipeline on caller-provided scratch: dens/dens_f hold (hermi ? nb :
 // 2nb) Cartesian matrices, vj nb, vk (hermi ? nb : 2nb); nothing is allocated
 // here when profiling is off.
@@ -1132,14 +1249,7 @@ void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j,
     CUDA_OK(cudaMemsetAsync(p.d_maxd.ptr, 0, sizeof(double), st));
     maxabs_kernel<<<592, 256, 0, st>>>(d_in, (long long)nb * p.out_stride, p.d_maxd.as<double>());
     CUDA_OK(cudaGetLastError());
-    for (auto* W : p.work)
-      for_each_unit(p, *W, [&](const JKUnit& u) {
-        if (u.nwork == 0) return;  // nothing of this class pair on this shard
-        split_kernel<<<(u.nwork + 127) / 128, 128, 0, st>>>(
-            u.work->as<int4>(), u.X->d_q.as<double>(), u.Y->d_q.as<double>(), p.d_maxd.as<double>(),
-            fp32_cut, u.nwork, u.split->as<int>());
-        CUDA_OK(cudaGetLastError());
-      });
+    for (auto* W : p.work) split_units(p, *W, fp32_cut, st);
   }
   JKArgs a = base_args(p);
   a.dens = s_dens;
@@ -1151,42 +1261,7 @@ void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j,
   a.nsym = nb;
   a.with_j = with_j;
   a.with_k = with_k;
-  const auto& disp = dispatch();
-  for (auto* W : p.work) {
-    const int cls = quartet_class(W->x, W->y);
-    for_each_unit(p, *W, [&](const JKUnit& u) {
-      if (u.nwork == 0) return;
-      set_unit_lists(a, u, W->x == W->y);
-      a.work = u.work->as<int4>();
-      a.nwork = u.nwork;
-      a.split = u.split->as<int>();
-      const bool plain = u.gb == 1 && u.gk == 1;
-      const JKLauncher l64 = plain ? disp.jk64[cls] : disp.jkg64[cls][gen_slot(u.gb, u.gk)];
-      const JKLauncher l32 = plain ? disp.jk32[cls] : disp.jkg32[cls][gen_slot(u.gb, u.gk)];
-      if (!l64 || !l32) throw Failure{B200JK_INTERNAL, "no kernel for this contraction grouping"};
-      auto launch = [&](int mode, bool fp32) {
-        a.split_mode = mode;
-        ProfileEvent ev{cls, fp32 ? 1 : 0, nullptr, nullptr};
-        if (p.profiling && allow_profiling) {
-          CUDA_OK(cudaEventCreate(&ev.start));
-          CUDA_OK(cudaEventCreate(&ev.stop));
-          CUDA_OK(cudaEventRecord(ev.start, st));
-        }
-        const int rc = fp32 ? l32(a, st) : l64(a, st);
-        if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
-        if (p.profiling && allow_profiling) {
-          CUDA_OK(cudaEventRecord(ev.stop, st));
-          p.events.push_back(ev);
-        }
-      };
-      if (precision == B200JK_FP64) {
-        launch(0, false);
-      } else {
-        launch(1, false);
-        launch(2, true);
-      }
-    });
-  }
+  for (auto* W : p.work) launch_units(p, *W, a, precision, st, allow_profiling);
   {
     const int no = max_no(p);
     const long long n2 = (long long)no * no;
@@ -1403,6 +1478,69 @@ int b200jk_partition_items(const int64_t* cost, int64_t n, int32_t world, int32_
   });
 }
 
+int b200jk_plan_autotune(b200jk_plan* plan, const double* d_density, int32_t nb, int32_t hermi,
+                         int32_t precision, double fp32_cut, int32_t reps, void* stream, int32_t* chunks) {
+  return guarded([&] {
+    if (!plan) invalid("Invalid plan");
+    if (reps < 1) invalid("autotune needs reps >= 1");
+    Plan& p = *plan->p;
+    cudaStream_t st = (cudaStream_t)stream;
+    check_jk_args(p, d_density, nb, d_density, 1, 1, precision, fp32_cut);
+    CUDA_OK(cudaSetDevice(p.device));
+    ensure_scratch(p, nb);
+    // one full build on the plan's scratch prepares the effective densities
+    // and the FP32 boundary input (max |D|); its result is discarded
+    DevBuf out;
+    CUDA_OK(out.ensure((size_t)2 * nb * p.out_stride * sizeof(double)));
+    run_jk_core(p, d_density, nb, out.as<double>(), 1, 1, hermi, precision, fp32_cut, st, p.d_dens.as<double>(),
+                p.d_dens_f.as<float>(), p.d_vj.as<double>(), p.d_vk.as<double>(), false);
+    JKArgs a = base_args(p);
+    a.dens = p.d_dens.as<double>();
+    a.dens_f = p.d_dens_f.as<float>();
+    a.vj = p.d_vj.as<double>();
+    a.vk = p.d_vk.as<double>();
+    a.dstride = p.cart_stride;
+    a.ndm = hermi ? nb : 2 * nb;
+    a.nsym = nb;
+    a.with_j = 1;
+    a.with_k = 1;
+    const auto& disp = dispatch();
+    cudaEvent_t e0, e1;
+    CUDA_OK(cudaEventCreate(&e0));
+    CUDA_OK(cudaEventCreate(&e1));
+    if (chunks) std::fill(chunks, chunks + kQuartetClasses, -1);
+    for (auto* W : p.work) {
+      const int cls = quartet_class(W->x, W->y);
+      if (!disp.reg_path[cls]) continue;  // tile / team items keep their sizes
+      int best = 0;
+      float best_ms = 0.f;
+      for (const int cand : {32, 64, 128}) {
+        fill_items(p, *W, cand);
+        apply_shard(p, *W);
+        if (precision == B200JK_SPLIT) split_units(p, *W, fp32_cut, st);
+        launch_units(p, *W, a, precision, st, false);  // warm-up
+        CUDA_OK(cudaEventRecord(e0, st));
+        for (int r = 0; r < reps; ++r) launch_units(p, *W, a, precision, st, false);
+        CUDA_OK(cudaEventRecord(e1, st));
+        CUDA_OK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
+        if (best == 0 || ms < best_ms) {
+          best = cand;
+          best_ms = ms;
+        }
+      }
+      fill_items(p, *W, best);
+      apply_shard(p, *W);
+      W->chunk = best;
+      if (chunks) chunks[cls] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CUDA_OK(cudaStreamSynchronize(st));
+  });
+}
+
 int b200jk_plan_set_shard(b200jk_plan* plan, int32_t rank, int32_t world) {
   return guarded([&] {
     if (!plan) invalid("Invalid plan");
@@ -1410,35 +1548,9 @@ int b200jk_plan_set_shard(b200jk_plan* plan, int32_t rank, int32_t world) {
     Plan& p = *plan->p;
     CUDA_OK(cudaSetDevice(p.device));
     CUDA_OK(cudaDeviceSynchronize());
-    // one partition per item list: the expanded items (coordinate VJP, and
-    // the J/K build of ungrouped class pairs) and every grouped bucket
-    auto shard = [&](const std::vector<int4>& all, const std::vector<int64_t>& cost, DevBuf& work,
-                     std::vector<int4>& h, int& nwork, long long& q, long long& pq, long long qmul) {
-      const int64_t n = (int64_t)all.size();
-      std::vector<int32_t> owner(n);
-      if (b200jk_partition_items(cost.data(), n, world, owner.data()) != 0)
-        throw Failure{B200JK_INTERNAL, "work-item partition failed"};
-      std::vector<int4> mine;
-      q = pq = 0;
-      for (int64_t i = 0; i < n; ++i) {
-        if (owner[i] != rank) continue;
-        mine.push_back(all[i]);
-        q += (long long)(all[i].z - all[i].y) * qmul;
-        pq += cost[i];
-      }
-      h = mine;
-      nwork = (int)mine.size();
-      if (!mine.empty())  // the buffer holds the full list, so it is never reallocated
-        CUDA_OK(cudaMemcpy(work.ptr, mine.data(), mine.size() * sizeof(int4), cudaMemcpyHostToDevice));
-    };
-    for (auto* W : p.work) {
-      shard(W->all_items, W->item_cost, W->work, W->h_items, W->nwork, W->quartets, W->prim_quartets, 1);
-      for (auto* B : W->buckets)
-        shard(B->all_items, B->item_cost, B->work, B->h_items, B->nwork, B->quartets, B->prim_quartets,
-              (long long)B->gb * B->gk);
-    }
     p.shard_rank = rank;
     p.shard_world = world;
+    for (auto* W : p.work) apply_shard(p, *W);
   });
 }
 

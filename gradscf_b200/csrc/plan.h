@@ -58,6 +58,7 @@ struct ClassPairWork {
   // grouped lists (contraction combinations shared): the J/K work is in
   // `buckets`; `work` still holds the expanded items (coordinate VJP)
   bool grouped_x = false, grouped_y = false;
+  int chunk = 0;                // register-path ket chunk chosen by the autotuner (0: default rule)
   std::vector<GenBucket*> buckets;
   ~ClassPairWork() {
     for (auto* b : buckets) delete b;

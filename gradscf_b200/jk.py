@@ -97,6 +97,22 @@ class DirectJKPlan:
         self.shard = (int(rank), int(world))
         self.group = group
 
+    def autotune(self, density, *, hermi=1, precision="split", fp32_cut=DEFAULT_FP32_CUT, reps=3, stream=None):
+        """Pick each register-path class pair's kets per work item (32, 64 or
+        128) by timing its kernels on `density` ((nb, packed_size), e.g. an SCF
+        iteration's dD); ``b200jk_plan_autotune``.  Returns {class: kets}.
+        Tune after ``set_shard`` and before creating a ``JKGraph``."""
+        d = density.reshape(-1, self.packed_size).contiguous()
+        if d.dtype != torch.float64 or d.device != self.device:
+            raise ValueError("density must be float64 on the plan's device")
+        chunks = (ctypes.c_int32 * _capi.NCLASS)()
+        with torch.cuda.device(self.device):
+            _capi.check(_capi.lib().b200jk_plan_autotune(
+                self._h, ctypes.c_void_p(d.data_ptr()), d.shape[0], int(bool(hermi)), PRECISIONS[precision],
+                float(fp32_cut), int(reps), _stream_handle(stream), chunks))
+        return {"({}{}|{}{})".format(*_capi.QUARTET_CLASSES[c]): chunks[c]
+                for c in range(_capi.NCLASS) if chunks[c] > 0}
+
     def reduce_shards(self, out):
         """Sum a sharded result over the ranks (in place); no-op when unsharded."""
         if self.shard[1] > 1:

@@ -86,6 +86,17 @@ int b200jk_plan_class_stats(const b200jk_plan* plan, int64_t* quartets, int64_t*
 int b200jk_partition_items(const int64_t* cost, int64_t n, int32_t world, int32_t* owner);
 int b200jk_plan_set_shard(b200jk_plan* plan, int32_t rank, int32_t world);
 
+/* Autotuner for the register-path tile shape (no counterpart in the
+ * reference, whose CPU loop has no tiles): for every class pair on the
+ * register path, times its kernels on `d_density` (nb packed matrices, the
+ * workload the plan will serve, e.g. an SCF iteration's dD) with 32, 64 and
+ * 128 kets per work item (`reps` timed launches after one warm-up each) and
+ * keeps the fastest.  chunks[55] (or NULL) receives the choice per class pair,
+ * -1 where not tuned.  Synchronises `stream`; call it before creating graphs
+ * (a graph keeps the work items it captured) and after set_shard. */
+int b200jk_plan_autotune(b200jk_plan* plan, const double* d_density, int32_t nb, int32_t hermi,
+                         int32_t precision, double fp32_cut, int32_t reps, void* stream, int32_t* chunks);
+
 /* After a B200JK_SPLIT call (synchronises `stream`): per class pair, the
  * quartets and primitive quartets that ran in FP64 and in FP32. */
 int b200jk_plan_split_stats(b200jk_plan* plan, void* stream, int64_t* q64, int64_t* q32,

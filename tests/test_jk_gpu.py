@@ -176,3 +176,18 @@ def test_sharded_partials_sum_to_full_build(precision):
     assert (acc - full).abs().max().item() < 1e-11
     again = plan.jk_packed(d, hermi=1, precision=precision)
     assert (again - full).abs().max().item() < 1e-12
+
+
+def test_autotune_keeps_results():
+    # the tuner only changes how kets are cut into work items: results are unchanged
+    from gradscf_b200 import workloads as W
+    top, par, sa, atm, bas, env = tables(W.water_cluster(3, 1), "cc-pvdz", False)
+    plan = J.DirectJKPlan([(atm, bas, env)], cart=False, cutoff=1e-12)
+    n = plan.nao[0]
+    d = torch.as_tensor(psd_density(n, 15, 6), device="cuda").reshape(1, -1)
+    ref = {p_: plan.jk_packed(d, hermi=1, precision=p_).clone() for p_ in ("fp64", "split")}
+    chosen = plan.autotune(d, precision="split", reps=1)
+    assert chosen and set(chosen.values()) <= {32, 64, 128}
+    for p_ in ("fp64", "split"):
+        got = plan.jk_packed(d, hermi=1, precision=p_)
+        assert (got - ref[p_]).abs().max().item() < 1e-11
