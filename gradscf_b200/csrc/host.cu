@@ -345,15 +345,87 @@ __global__ void maxabs_kernel(const double* __restrict__ x, long long n, double*
     atomicMax(reinterpret_cast<unsigned long long*>(out), (unsigned long long)__double_as_longlong(m));
 }
 
+// max |D| over every row of the effective Cartesian densities (all sets), by
+// global Cartesian row; one warp per row.
+__global__ void rowmax_kernel(const double* __restrict__ dens, int ndm, long long dstride,
+                              const long long* __restrict__ mol_base, const int* __restrict__ mol_n,
+                              const int* __restrict__ mol_ao_off, const int* __restrict__ cart_ws,
+                              const int4* __restrict__ ws_info, int nrows, double* __restrict__ rowmax) {
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= nrows) return;
+  const int m = ws_info[cart_ws[row]].z;
+  const int n = mol_n[m];
+  const long long base = mol_base[m] + (long long)(row - mol_ao_off[m]) * n;
+  double v = 0.0;
+  for (int e = 0; e < ndm; ++e)
+    for (int j = lane; j < n; j += 32) v = fmax(v, fabs(dens[e * dstride + base + j]));
+  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+  if (lane == 0) rowmax[row] = v;
+}
+
+// Density bound of the quartets of one work item: every density element a
+// quartet (ab|cd) digests (D_cd, D_ab, D_bd, D_bc, D_ad, D_ac) lies in a row
+// of shell A, B or C, so max |D| over those rows bounds them; over the
+// item's kets (and every contraction combination of grouped entries).
+struct SplitLists {
+  const int4 *bix, *bgx, *bgy;
+  const double* kmax;  // per ket position: max |D| over its C rows
+  const double4* bra;
+  int gb, na, nb;
+};
+
+__device__ __forceinline__ double rows_max(const double* rowmax, int base, int off, int n) {
+  double v = 0.0;
+  for (int i = 0; i < n; ++i) v = fmax(v, rowmax[base + off + i]);
+  return v;
+}
+
+// Per list position: max |D| over the rows of its A shell (every combination).
+__global__ void posmax_kernel(const int4* __restrict__ ix, const int4* __restrict__ gx,
+                              const int4* __restrict__ gy, const int* __restrict__ nco,
+                              const double4* __restrict__ ra, int npos, int na,
+                              const double* __restrict__ rowmax, const int* __restrict__ mol_ao_off,
+                              double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npos) return;
+  const int base = mol_ao_off[(int)ra[k].w];
+  const int g = nco ? nco[k] : 1;
+  double v = rows_max(rowmax, base, ix[k].z, na);
+  if (g > 1) {
+    const int4 x = gx[k], y = gy[k];
+    v = fmax(v, rows_max(rowmax, base, x.z, na));
+    if (g > 2) v = fmax(v, fmax(rows_max(rowmax, base, y.x, na), rows_max(rowmax, base, y.z, na)));
+  }
+  out[k] = v;
+}
+
 // Per work item: first ket position of its range computed in FP32,
-// Q_bra * Q_ket * max|D| < fp32_cut (ket bounds sorted descending).
+// Q_bra * Q_ket * max|D over the rows the item's quartets touch| < fp32_cut
+// (ket bounds sorted descending, so the FP32 kets are a suffix).
 __global__ void split_kernel(const int4* __restrict__ work, const double* __restrict__ bra_q,
-                             const double* __restrict__ ket_q, const double* maxd, double fp32_cut,
+                             const double* __restrict__ ket_q, const double* __restrict__ rowmax,
+                             const int* __restrict__ mol_ao_off, SplitLists L, double fp32_cut,
                              int nwork, int* __restrict__ split) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  // one warp per item: the lanes take the item's kets, then lane 0 searches
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   if (i >= nwork) return;
   const int4 w = work[i];
-  const double f = bra_q[w.x] * (*maxd);
+  const int base = mol_ao_off[(int)L.bra[w.x].w];
+  double dmax = 0.0;
+  if (lane < L.gb) {
+    const int4 ix = L.bix[w.x];
+    const int4 gx = L.gb > 1 ? L.bgx[w.x] : make_int4(0, 0, 0, 0);
+    const int4 gy = L.gb > 1 ? L.bgy[w.x] : make_int4(0, 0, 0, 0);
+    const int a = lane == 0 ? ix.z : lane == 1 ? gx.z : lane == 2 ? gy.x : gy.z;
+    const int b = lane == 0 ? ix.w : lane == 1 ? gx.w : lane == 2 ? gy.y : gy.w;
+    dmax = fmax(rows_max(rowmax, base, a, L.na), rows_max(rowmax, base, b, L.nb));
+  }
+  for (int k = w.y + lane; k < w.z; k += 32) dmax = fmax(dmax, L.kmax[k]);
+  for (int off = 16; off > 0; off >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, off));
+  if (lane != 0) return;
+  const double f = bra_q[w.x] * dmax;
   int lo = w.y, hi = w.z;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
@@ -365,6 +437,7 @@ __global__ void split_kernel(const int4* __restrict__ work, const double* __rest
 
 // ---------------------------------------------------------------- plan creation
 static int ncart_of(int l) { return (l + 1) * (l + 2) / 2; }
+static int pc_la_host(int pc) { return pc == 0 ? 0 : pc <= 2 ? 1 : pc <= 5 ? 2 : 3; }
 
 struct PrimPair {
   double4 data;
@@ -898,6 +971,7 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
       o += p.mol_nout[m];
     }
     upload(p.d_mol_ao_off, v.data(), v.size() * sizeof(int));
+    CUDA_OK(p.d_rowmax.ensure((size_t)std::max(c, 1) * sizeof(double)));
   }
   CUDA_OK(p.d_q_work.ensure(std::max(p.npair, 1) * sizeof(double)));
   {
@@ -991,6 +1065,7 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     upload(L.d_ra, ra.data(), ra.size() * sizeof(double4));
     upload(L.d_ab, ab.data(), ab.size() * sizeof(double4));
     upload(L.d_ix, ix.data(), ix.size() * sizeof(int4));
+    CUDA_OK(L.d_kmax.ensure(std::max<size_t>(ids.size(), 1) * sizeof(double)));
   }
   // the combinations of the grouped entries cover exactly the expanded
   // work pairs of their classes (checked once per plan, on the host)
@@ -1078,6 +1153,8 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     upload(L.d_ix, ix.data(), n * sizeof(int4));
     upload(L.d_gx, gx.data(), n * sizeof(int4));
     upload(L.d_gy, gy.data(), n * sizeof(int4));
+    upload(L.d_nco, L.nco.data(), n * sizeof(int));
+    CUDA_OK(L.d_kmax.ensure(std::max<size_t>(n, 1) * sizeof(double)));
   }
   // ---- work items per class pair (X >= Y)
   for (int x = 0; x < kPairClasses; ++x)
@@ -1168,13 +1245,19 @@ void check_jk_args(const Plan& p, const double* d_in, int nb, const double* d_ou
   if (!d_in || !d_out) invalid("Null density or output pointer");
 }
 
-// The FP32/FP64 boundary of every item of class pair W (split mode).
+// The FP32/FP64 boundary of every item of class pair W (split mode); the
+// row maxima of the effective densities are in p.d_rowmax.
 static void split_units(Plan& p, ClassPairWork& W, double fp32_cut, cudaStream_t st) {
+  const int la = pc_la_host(W.x), lb = W.x - la * (la + 1) / 2, lc = pc_la_host(W.y);
   for_each_unit(p, W, [&](const JKUnit& u) {
     if (u.nwork == 0) return;  // nothing of this class pair on this shard
-    split_kernel<<<(u.nwork + 127) / 128, 128, 0, st>>>(u.work->as<int4>(), u.X->d_q.as<double>(),
-                                                       u.Y->d_q.as<double>(), p.d_maxd.as<double>(),
-                                                       fp32_cut, u.nwork, u.split->as<int>());
+    (void)lc;
+    SplitLists L{u.X->d_ix.as<int4>(), u.X->d_gx.as<int4>(), u.X->d_gy.as<int4>(), u.Y->d_kmax.as<double>(),
+                 u.X->d_ra.as<double4>(), u.gb, ncart_of(la), ncart_of(lb)};
+    split_kernel<<<(u.nwork + 3) / 4, 128, 0, st>>>(u.work->as<int4>(), u.X->d_q.as<double>(),
+                                                       u.Y->d_q.as<double>(), p.d_rowmax.as<double>(),
+                                                       p.d_mol_ao_off.as<int>(), L, fp32_cut, u.nwork,
+                                                       u.split->as<int>());
     CUDA_OK(cudaGetLastError());
   });
 }
@@ -1249,6 +1332,22 @@ void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j,
     CUDA_OK(cudaMemsetAsync(p.d_maxd.ptr, 0, sizeof(double), st));
     maxabs_kernel<<<592, 256, 0, st>>>(d_in, (long long)nb * p.out_stride, p.d_maxd.as<double>());
     CUDA_OK(cudaGetLastError());
+    const int nrows = (int)(p.d_rowmax.bytes / sizeof(double));
+    rowmax_kernel<<<(nrows + 7) / 8, 256, 0, st>>>(s_dens, ndm, p.cart_stride, p.d_mol_base_cart.as<long long>(),
+                                                  p.d_mol_ncart.as<int>(), p.d_mol_ao_off.as<int>(),
+                                                  p.d_cart_ws.as<int>(), p.d_ws_info.as<int4>(), nrows,
+                                                  p.d_rowmax.as<double>());
+    CUDA_OK(cudaGetLastError());
+    for (int c = 0; c < kPairClasses; ++c)
+      for (ClassList* Lp : {&p.classes[c], &p.grouped[c]}) {
+        const int npos = (int)Lp->q.size();
+        if (npos == 0) continue;
+        posmax_kernel<<<(npos + 127) / 128, 128, 0, st>>>(
+            Lp->d_ix.as<int4>(), Lp->d_gx.as<int4>(), Lp->d_gy.as<int4>(), Lp->d_nco.as<int>(),
+            Lp->d_ra.as<double4>(), npos, ncart_of(pc_la_host(c)), p.d_rowmax.as<double>(),
+            p.d_mol_ao_off.as<int>(), Lp->d_kmax.as<double>());
+        CUDA_OK(cudaGetLastError());
+      }
     for (auto* W : p.work) split_units(p, *W, fp32_cut, st);
   }
   JKArgs a = base_args(p);
