@@ -1888,8 +1888,18 @@ int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_
       a.work = W->work.as<int4>();
       a.nwork = W->nwork;
       a.split_mode = 0;
+      ProfileEvent ev{cls, 0, nullptr, nullptr};  // profiling: gradient launches count as FP64
+      if (p.profiling) {
+        CUDA_OK(cudaEventCreate(&ev.start));
+        CUDA_OK(cudaEventCreate(&ev.stop));
+        CUDA_OK(cudaEventRecord(ev.start, st));
+      }
       const int rc = disp.grad64[cls](a, st);
       if (rc) throw Failure{B200JK_INTERNAL, std::string("gradient launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+      if (p.profiling) {
+        CUDA_OK(cudaEventRecord(ev.stop, st));
+        p.events.push_back(ev);
+      }
     }
   });
 }
