@@ -268,9 +268,6 @@ def main():
             lib.b200jk_plan_set_profiling(plan._h, 0)
             ms64 = (ctypes.c_double * nc)(); ms32 = (ctypes.c_double * nc)(); nl = (ctypes.c_int32 * nc)()
             _capi.check(lib.b200jk_plan_profile(plan._h, ms64, ms32, nl))
-            ev64 = (ctypes.c_int64 * nc)(); ev32 = (ctypes.c_int64 * nc)()
-            _capi.check(lib.b200jk_plan_prim_counts(plan._h, ev64, ev32))
-            acc["ev64"], acc["ev32"] = np.array(list(ev64), float), np.array(list(ev32), float)
             if dist:
                 t = torch.tensor([step_ms], device=dev)
                 dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -324,11 +321,7 @@ def main():
             t = results["split"][msk][c]
             if t <= 0:
                 continue
-            # primitive quartets actually evaluated (after FP32 primitive
-            # screening) where the kernel counts them (register path)
-            evk = "ev64" if kind == "fp64" else "ev32"
-            npq = acc[evk][c] if acc[evk][c] > 0 else acc[pqk][c]
-            fl = flop_model.class_flops(classes[c], npq, acc[qk][c])
+            fl = flop_model.class_flops(classes[c], acc[pqk][c], acc[qk][c])
             top.append({"class": "(%d%d|%d%d)" % classes[c], "prec": kind, "ms_per_step": round(t / K, 3),
                         "tflops": round(fl / (t * 1e-3) / 1e12, 3) if fl else 0.0})
             if best is None or t > best[0]:
@@ -366,8 +359,6 @@ def main():
                        "abs_dE_hartree": abs(r32.energy - r64.energy),
                        "last_iter_dE_fp64": abs(r64.energies[-1] - r64.energies[-2])},
             "split_fraction_fp32_quartets": float(acc["q32"].sum() / max(1.0, acc["q32"].sum() + acc["q64"].sum())),
-            "fp32_primitive_quartets_evaluated_frac": float(
-                acc["ev32"].sum() / max(1.0, sum(acc["pq32"][c_] for c_ in range(nc) if acc["ev32"][c_] > 0))),
             "max_abs_dD_timed": [float(x) for x in acc["maxdd"]],
             "e2e": {"value": quartets / (e2e_step * 1e-3), "unit": "quartets/s",
                     "ms_per_step": e2e_step, "h2d_bytes_per_step": int(n * n * 8),

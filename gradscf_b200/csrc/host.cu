@@ -526,8 +526,6 @@ static void set_unit_lists(JKArgs& a, const JKUnit& u, bool same) {
   a.ket_ix = u.Y->d_ix.as<int4>();
   a.ket_gx = u.Y->d_gx.as<int4>();
   a.ket_gy = u.Y->d_gy.as<int4>();
-  a.bra_q = u.X->d_q.as<double>();
-  a.ket_q = u.Y->d_q.as<double>();
   a.same_list = same;
 }
 
@@ -547,11 +545,6 @@ static JKArgs base_args(const Plan& p) {
   a.pp_f = p.d_pp_f.as<float4>();
   a.pp_f2 = p.d_pp_f2.as<float2>();
   a.pp_c = p.d_pp_c.as<double4>();
-  a.pp_q = p.d_pp_q.as<float>();
-#ifndef B200JK_PRIM_REL
-#define B200JK_PRIM_REL 5.9604645e-8   // 2^-24: below FP32 resolution of the quartet's bound
-#endif
-  a.prim_rel = (float)(B200JK_PRIM_REL);
   a.pp_cf = p.d_pp_cf.as<float4>();
   a.ws_atm = p.d_ws_atm.as<int>();
   a.mol_base = p.d_mol_base_cart.as<long long>();
@@ -994,76 +987,6 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     }
     CUDA_OK(cudaDeviceSynchronize());
   }
-  // ---- primitive-level Schwarz factors: sqrt(max |(ab|ab)|) of every
-  // primitive pair alone (times its largest combination coefficient), for
-  // the FP32 path's primitive screening; primitives are then sorted by it
-  // within every pair so both primitive loops can stop early
-  {
-    const size_t npp_all = pp_data.size();
-    std::vector<int4> pseudo(npp_all);
-    std::vector<std::vector<int>> pcls(kPairClasses);
-    auto add_range = [&](int A, int B, int off, int cnt, int c) {
-      for (int i = off; i < off + cnt; ++i) {
-        pseudo[i] = make_int4(A, B, i, 1);
-        pcls[c].push_back(i);
-      }
-    };
-    for (int q = 0; q < p.npair; ++q)
-      add_range(p.pair_info[q].x, p.pair_info[q].y, p.pair_info[q].z, p.pair_info[q].w, p.pair_class[q]);
-    for (const GenEntry& e : gen)
-      if (e.pair < 0) add_range(e.ws[0], e.wsb[0], e.ppoff, e.npp, e.cls);
-    DevBuf d_pseudo, d_qp;
-    upload(d_pseudo, pseudo.data(), npp_all * sizeof(int4));
-    CUDA_OK(d_qp.ensure(std::max<size_t>(npp_all, 1) * sizeof(double)));
-    for (int c = 0; c < kPairClasses; ++c) {
-      if (pcls[c].empty()) continue;
-      DevBuf lst;
-      upload(lst, pcls[c].data(), pcls[c].size() * sizeof(int));
-      JKArgs a = base_args(p);
-      a.pair_info = d_pseudo.as<int4>();
-      a.bra_pairs = lst.as<int>();
-      a.q_out = d_qp.as<double>();
-      const int rc = dispatch().schwarz[c](a, (int)pcls[c].size(), cart, 0);
-      if (rc) throw Failure{B200JK_INTERNAL, std::string("primitive Schwarz launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
-      CUDA_OK(cudaDeviceSynchronize());
-    }
-    std::vector<double> qp(npp_all);
-    if (npp_all) CUDA_OK(cudaMemcpy(qp.data(), d_qp.ptr, npp_all * sizeof(double), cudaMemcpyDeviceToHost));
-    std::vector<float> qf(npp_all);
-    for (size_t i = 0; i < npp_all; ++i) {
-      const double4 c = pp_c[i];
-      const double cmax = std::max(std::max(std::fabs(c.x), std::fabs(c.y)), std::max(std::fabs(c.z), std::fabs(c.w)));
-      qf[i] = float(std::sqrt(std::max(qp[i], 0.0)) * cmax);
-    }
-    // sort every pair's primitive range by the factor, descending
-    std::vector<int> order;
-    auto sort_range = [&](int off, int cnt) {
-      order.resize(cnt);
-      for (int i = 0; i < cnt; ++i) order[i] = off + i;
-      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return qf[a] > qf[b]; });
-      auto permute = [&](auto& v) {
-        std::vector<std::decay_t<decltype(v[0])>> tmp(cnt);
-        for (int i = 0; i < cnt; ++i) tmp[i] = v[order[i]];
-        for (int i = 0; i < cnt; ++i) v[off + i] = tmp[i];
-      };
-      permute(pp_data); permute(pp_aux); permute(pp_exp); permute(pp_f); permute(pp_f2); permute(pp_c);
-      permute(qf);
-    };
-    for (int q = 0; q < p.npair; ++q) sort_range(p.pair_info[q].z, p.pair_info[q].w);
-    for (const GenEntry& e : gen)
-      if (e.pair < 0) sort_range(e.ppoff, e.npp);
-    upload(p.d_pp_data, pp_data.data(), pp_data.size() * sizeof(double4));
-    upload(p.d_pp_aux, pp_aux.data(), pp_aux.size() * sizeof(double2));
-    upload(p.d_pp_exp, pp_exp.data(), pp_exp.size() * sizeof(double2));
-    upload(p.d_pp_f, pp_f.data(), pp_f.size() * sizeof(float4));
-    upload(p.d_pp_f2, pp_f2.data(), pp_f2.size() * sizeof(float2));
-    std::vector<float4> pp_cf(pp_c.size());
-    for (size_t i = 0; i < pp_c.size(); ++i)
-      pp_cf[i] = make_float4(float(pp_c[i].x), float(pp_c[i].y), float(pp_c[i].z), float(pp_c[i].w));
-    upload(p.d_pp_c, pp_c.data(), pp_c.size() * sizeof(double4));
-    upload(p.d_pp_cf, pp_cf.data(), pp_cf.size() * sizeof(float4));
-    upload(p.d_pp_q, qf.data(), qf.size() * sizeof(float));
-  }
   std::vector<double> qw(p.npair);
   if (p.npair) CUDA_OK(cudaMemcpy(qw.data(), p.d_q_work.ptr, p.npair * sizeof(double), cudaMemcpyDeviceToHost));
   // parent-pair bound: max over the work pairs of the parent pair
@@ -1357,8 +1280,6 @@ static void launch_units(Plan& p, ClassPairWork& W, JKArgs a, int precision, cud
     if (!l64 || !l32) throw Failure{B200JK_INTERNAL, "no kernel for this contraction grouping"};
     auto launch = [&](int mode, bool fp32) {
       a.split_mode = mode;
-      const bool prof = p.profiling && allow_profiling;
-      a.prim_count = prof ? p.d_prim_count.as<unsigned long long>() + 2 * cls + (fp32 ? 1 : 0) : nullptr;
       ProfileEvent ev{cls, fp32 ? 1 : 0, nullptr, nullptr};
       if (p.profiling && allow_profiling) {
         CUDA_OK(cudaEventCreate(&ev.start));
@@ -1907,31 +1828,7 @@ int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_
 int b200jk_plan_set_profiling(b200jk_plan* plan, int32_t on) {
   return guarded([&] {
     if (!plan) invalid("Null plan");
-    Plan& p = *plan->p;
-    if (on && !p.profiling) {
-      CUDA_OK(cudaSetDevice(p.device));
-      CUDA_OK(p.d_prim_count.ensure(2 * kQuartetClasses * sizeof(unsigned long long)));
-      CUDA_OK(cudaMemset(p.d_prim_count.ptr, 0, 2 * kQuartetClasses * sizeof(unsigned long long)));
-    }
-    p.profiling = on != 0;
-  });
-}
-
-int b200jk_plan_prim_counts(b200jk_plan* plan, int64_t* ev64, int64_t* ev32) {
-  return guarded([&] {
-    if (!plan || !ev64 || !ev32) invalid("Invalid plan query");
-    Plan& p = *plan->p;
-    CUDA_OK(cudaSetDevice(p.device));
-    std::vector<unsigned long long> h(2 * kQuartetClasses, 0);
-    if (p.d_prim_count.ptr) {
-      CUDA_OK(cudaDeviceSynchronize());
-      CUDA_OK(cudaMemcpy(h.data(), p.d_prim_count.ptr, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-      CUDA_OK(cudaMemset(p.d_prim_count.ptr, 0, h.size() * sizeof(unsigned long long)));
-    }
-    for (int c = 0; c < kQuartetClasses; ++c) {
-      ev64[c] = (int64_t)h[2 * c];
-      ev32[c] = (int64_t)h[2 * c + 1];
-    }
+    plan->p->profiling = on != 0;
   });
 }
 

@@ -38,10 +38,6 @@ struct JKArgs {
   const int4 *bra_ix, *ket_ix;
   // grouped lists: (diag, 0, aoA1, aoB1), (aoA2, aoB2, aoA3, aoB3) per position
   const int4 *bra_gx, *bra_gy, *ket_gx, *ket_gy;
-  const float* pp_q;         // per primitive pair: primitive Schwarz factor (sorted descending per pair)
-  const double *bra_q, *ket_q;  // per list position: contracted Schwarz bound Q
-  float prim_rel;            // FP32 quartets skip primitive quartets with q_i q_j < prim_rel Q_bra Q_ket
-  unsigned long long* prim_count;  // profiling: primitive quartets evaluated (null: not counted)
   const double4* pp_c;       // per primitive pair: coefficients of up to 4 combinations
   const float4* pp_cf;       // the same in FP32
   int same_list;
@@ -286,14 +282,11 @@ __device__ __forceinline__ long long dm_index(const JKArgs& args, int mol, int a
 #define B200JK_REG_UNROLL 2
 #endif
 constexpr int kRegUnroll = B200JK_REG_UNROLL;   // bra primitives interleaved per step (ILP)
-// FP32 primitive screening: primitives are sorted by their Schwarz factor q
-// within a pair, so once q_i q_j < tau the rest of a loop is below it too.
 template <int LA, int LB, int LC, int LD, typename R>
 __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const QuartetGeom& g,
                                                   const typename PrimData<R>::A* bpp,
                                                   const typename PrimData<R>::B* baux, R* out,
-                                                  const float* s_boys, const float* bq, float tau,
-                                                  int& evaluated) {
+                                                  const float* s_boys) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   using GI = GIdx<LA, LB, LC, LD>;
   constexpr int N = CI::NROOT;
@@ -305,30 +298,15 @@ __device__ __forceinline__ void quartet_block_reg(const JKArgs& args, const Quar
   // the next ket primitive is fetched while the current one is in use
   auto Qn = PrimData<R>::a(args, g.ppc);
   auto QAn = PrimData<R>::b(args, g.ppc);
-  float qn = sizeof(R) == 4 ? args.pp_q[g.ppc] : 0.f;
   for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
     const auto Q = Qn;
     const auto QA = QAn;
-    const float qj = qn;
     if (j + 1 < g.ppc + g.npc) {
       Qn = PrimData<R>::a(args, j + 1);
       QAn = PrimData<R>::b(args, j + 1);
-      if constexpr (sizeof(R) == 4) qn = args.pp_q[j + 1];
     }
-    int nbra = g.npa;
-    if constexpr (sizeof(R) == 4) {
-      if (bq[0] * qj < tau) break;
-      int lo = 1, hi = g.npa;  // first bra primitive below tau (sorted descending)
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (bq[mid] * qj < tau) hi = mid;
-        else lo = mid + 1;
-      }
-      nbra = lo;
-    }
-    evaluated += nbra;
 #pragma unroll(kRegUnroll)
-    for (int i = 0; i < nbra; ++i) {
+    for (int i = 0; i < g.npa; ++i) {
       PrimQ<R> s;
       prim_any<R>(g, ac, bpp[i], baux[i], Q, QA, s);
       R x[N], w[N];
@@ -554,7 +532,6 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
   using PB_t = typename PrimData<R>::B;
   __shared__ PA_t s_pp[kRegWarps][kBraPrimCache];
   __shared__ PB_t s_aux[kRegWarps][kBraPrimCache];
-  __shared__ float s_bq[kRegWarps][kBraPrimCache];
   __shared__ double s_jab[kRegWarps][CI::NAB];
   // FP32 path with closed-form roots: this order's Taylor table (12.8 KB)
   constexpr bool kSharedBoys = sizeof(R) == 4 && CI::NROOT <= 3;
@@ -583,10 +560,7 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
     for (int i = lane; i < npb; i += 32) {
       s_pp[warp][i] = PrimData<R>::a(args, ppb + i);
       s_aux[warp][i] = PrimData<R>::b(args, ppb + i);
-      s_bq[warp][i] = args.pp_q[ppb + i];
     }
-  const float* bq = cached ? s_bq[warp] : args.pp_q + ppb;
-  const double qbra = args.bra_q[w.x];
   const bool acc_j = args.with_j && args.nsym == 1;
   for (int i = lane; i < CI::NAB; i += 32) s_jab[warp][i] = 0.0;
   __syncwarp();
@@ -595,7 +569,6 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
   const PB_t* baux = cached ? s_aux[warp] : (sizeof(R) == 4 ? (const PB_t*)(args.pp_f2 + ppb)
                                                            : (const PB_t*)(args.pp_aux + ppb));
   QuartetGeom g;
-  long long evaluated = 0;  // primitive quartets evaluated by this lane (profiling count)
   for (int k0 = kb; k0 < ke; k0 += 32) {
     // lanes past the range recompute the last ket with their output masked,
     // so the whole warp takes part in the J shuffles
@@ -605,15 +578,8 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
     DensPre<LA, LB, LC, LD, R> pre;
     pre.load(args, g);
     R out[CI::NOUT];
-    const float tau = sizeof(R) == 4 ? float(args.prim_rel * qbra * args.ket_q[k]) : 0.f;
-    int ev = 0;
-    quartet_block_reg<LA, LB, LC, LD, R>(args, g, bpp, baux, out, s_boys, bq, tau, ev);
-    if (active) evaluated += ev;
+    quartet_block_reg<LA, LB, LC, LD, R>(args, g, bpp, baux, out, s_boys);
     digest_reg<LA, LB, LC, LD, R>(args, g, out, acc_j, active, s_jab[warp], pre);
-  }
-  if (args.prim_count) {
-    for (int off = 16; off > 0; off >>= 1) evaluated += __shfl_down_sync(0xffffffffu, evaluated, off);
-    if (lane == 0) atomicAdd(args.prim_count, (unsigned long long)evaluated);
   }
   if (acc_j) {
     __syncwarp();
@@ -658,8 +624,7 @@ __device__ __forceinline__ void quartet_block_gen(const JKArgs& args, const Quar
                                                   const typename PrimData<R>::A* bpp,
                                                   const typename PrimData<R>::B* baux,
                                                   const typename CoefSel<R>::T* bco, R* out,
-                                                  const float* s_boys, const float* bq, float tau,
-                                                  int& evaluated) {
+                                                  const float* s_boys) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   using GI = GIdx<LA, LB, LC, LD>;
   constexpr int N = CI::NROOT, NO = CI::NOUT;
@@ -669,31 +634,16 @@ __device__ __forceinline__ void quartet_block_gen(const JKArgs& args, const Quar
   auto Qn = PrimData<R>::a(args, g.ppc);
   auto QAn = PrimData<R>::b(args, g.ppc);
   auto Cn = CoefSel<R>::get(args, g.ppc);
-  float qn = sizeof(R) == 4 ? args.pp_q[g.ppc] : 0.f;
   for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
     const auto Q = Qn;
     const auto QA = QAn;
     const auto CK = Cn;
-    const float qj = qn;
     if (j + 1 < g.ppc + g.npc) {
       Qn = PrimData<R>::a(args, j + 1);
       QAn = PrimData<R>::b(args, j + 1);
       Cn = CoefSel<R>::get(args, j + 1);
-      if constexpr (sizeof(R) == 4) qn = args.pp_q[j + 1];
     }
-    int nbra = g.npa;
-    if constexpr (sizeof(R) == 4) {
-      if (bq[0] * qj < tau) break;
-      int lo = 1, hi = g.npa;  // first bra primitive below tau (sorted descending)
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (bq[mid] * qj < tau) hi = mid;
-        else lo = mid + 1;
-      }
-      nbra = lo;
-    }
-    evaluated += nbra;
-    for (int i = 0; i < nbra; ++i) {
+    for (int i = 0; i < g.npa; ++i) {
       PrimQ<R> s;
       prim_any<R>(g, ac, bpp[i], baux[i], Q, QA, s);
       R x[N], w[N];
@@ -752,7 +702,6 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
   __shared__ PA_t s_pp[kRegWarps][kBraPrimCache];
   __shared__ PB_t s_aux[kRegWarps][kBraPrimCache];
   __shared__ C4 s_co[kRegWarps][kBraPrimCache];
-  __shared__ float s_bq[kRegWarps][kBraPrimCache];
   __shared__ double s_jab[kRegWarps][GB * CI::NAB];
   constexpr bool kSharedBoys = sizeof(R) == 4 && CI::NROOT <= 3;
   __shared__ __align__(16) float s_boys[kSharedBoys ? 401 * 8 : 4];
@@ -795,10 +744,7 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
       s_pp[warp][i] = PrimData<R>::a(args, ppb + i);
       s_aux[warp][i] = PrimData<R>::b(args, ppb + i);
       s_co[warp][i] = CoefSel<R>::get(args, ppb + i);
-      s_bq[warp][i] = args.pp_q[ppb + i];
     }
-  const float* bq = cached ? s_bq[warp] : args.pp_q + ppb;
-  const double qbra = args.bra_q[w.x];
   const bool acc_j = args.with_j && args.nsym == 1;
   for (int i = lane; i < GB * CI::NAB; i += 32) s_jab[warp][i] = 0.0;
   __syncwarp();
@@ -809,7 +755,6 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
   const C4* bco = cached ? s_co[warp] : (sizeof(R) == 4 ? (const C4*)(args.pp_cf + ppb)
                                                        : (const C4*)(args.pp_c + ppb));
   QuartetGeom g;
-  long long evaluated = 0;
   for (int k0 = kb; k0 < ke; k0 += 32) {
     const bool active = k0 + lane < ke;
     const int k = active ? k0 + lane : ke - 1;
@@ -829,10 +774,7 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
     }
     const double sbk = (bdiag ? 0.5 : 1.0) * (kdiag ? 0.5 : 1.0) * (args.same_list && k == w.x ? 0.5 : 1.0);
     R out[GB * GK * NO];
-    const float tau = sizeof(R) == 4 ? float(args.prim_rel * qbra * args.ket_q[k]) : 0.f;
-    int ev = 0;
-    quartet_block_gen<LA, LB, LC, LD, R, GB, GK>(args, g, bpp, baux, bco, out, s_boys, bq, tau, ev);
-    if (active) evaluated += ev;
+    quartet_block_gen<LA, LB, LC, LD, R, GB, GK>(args, g, bpp, baux, bco, out, s_boys);
 #pragma unroll
     for (int b = 0; b < GB; ++b)
 #pragma unroll
@@ -845,10 +787,6 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
         digest_reg<LA, LB, LC, LD, R>(args, gc, out + (b * GK + c) * NO, acc_j, active,
                                       s_jab[warp] + b * CI::NAB, pre);
       }
-  }
-  if (args.prim_count) {
-    for (int off = 16; off > 0; off >>= 1) evaluated += __shfl_down_sync(0xffffffffu, evaluated, off);
-    if (lane == 0) atomicAdd(args.prim_count, (unsigned long long)evaluated);
   }
   if (acc_j) {
     __syncwarp();

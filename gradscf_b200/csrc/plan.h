@@ -124,9 +124,7 @@ struct Plan {
   std::vector<double4> atom_xyzq; // (x, y, z, charge) per global atm row
   // device tables
   DevBuf d_pp_c, d_pp_cf;          // per primitive pair: combination coefficients (FP64, FP32)
-  DevBuf d_pp_q;                   // per primitive pair: primitive Schwarz factor (FP32 screening)
-  DevBuf d_rowmax;
-  DevBuf d_prim_count;             // profiling: evaluated primitive quartets per class pair and precision                 // per Cartesian row (all molecules): max |D| of the last split call
+  DevBuf d_rowmax;                 // per Cartesian row (all molecules): max |D| of the last split call
   DevBuf d_ws_info, d_ws_xyz, d_pair_info, d_pp_data, d_pp_aux, d_pp_exp, d_pp_f, d_pp_f2, d_mol_base_cart, d_mol_ncart,
       d_mol_base_out, d_mol_nout, d_cart_ws, d_out_ws, d_status, d_maxd, d_q_work, d_atoms,
       d_ws_atm, d_mol_ao_off, d_ws_prim, d_ws_prim_off;

@@ -108,11 +108,6 @@ int b200jk_plan_split_stats(b200jk_plan* plan, void* stream, int64_t* q64, int64
  * the last read, then resets. */
 int b200jk_plan_set_profiling(b200jk_plan* plan, int32_t on);
 int b200jk_plan_profile(b200jk_plan* plan, double* ms64, double* ms32, int32_t* launches);
-/* Primitive quartets the register-path kernels evaluated per class pair
- * (FP64 and FP32 launches) while profiling was on -- after FP32 primitive
- * screening; synchronises the device, returns the counts since the last
- * read, then resets.  Classes on the tile / team paths count 0. */
-int b200jk_plan_prim_counts(b200jk_plan* plan, int64_t* ev64, int64_t* ev32);
 
 /* Measured vector-pipe FMA throughput of the current device in TFLOP/s
  * (fp64 = 1: FP64, 0: FP32) -- the roofline denominator for the ERI kernels. */
