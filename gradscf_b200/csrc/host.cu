@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <unordered_map>
 #include <set>
 #include <functional>
 #include <memory>
@@ -507,9 +508,11 @@ static void for_each_unit(Plan& p, ClassPairWork& W, F&& f) {
   if (!W.buckets.empty()) {
     const ClassList* X = W.grouped_x ? &p.grouped[W.x] : &p.classes[W.x];
     const ClassList* Y = W.grouped_y ? &p.grouped[W.y] : &p.classes[W.y];
-    for (auto* B : W.buckets) f(JKUnit{&B->work, B->nwork, &B->split, X, Y, B->gb, B->gk, &B->h_items});
+    for (auto* B : W.buckets)
+      f(JKUnit{&B->work, B->nwork, &B->split, X, Y, B->gb, B->gk, B->h_items.empty() ? &B->all_items : &B->h_items});
   } else {
-    f(JKUnit{&W.work, W.nwork, &W.split, &p.classes[W.x], &p.classes[W.y], 1, 1, &W.h_items});
+    f(JKUnit{&W.work, W.nwork, &W.split, &p.classes[W.x], &p.classes[W.y], 1, 1,
+             W.h_items.empty() ? &W.all_items : &W.h_items});
   }
 }
 
@@ -636,8 +639,8 @@ static void fill_items(Plan& p, ClassPairWork& W, int force) {
   });
   W.nwork = (int)items.size();
   upload_items(W.work, W.split, items);
-  W.h_items = items;
-  W.all_items = items;
+  W.h_items.clear();  // unsharded: the active items are all_items
+  W.all_items = std::move(items);
   for (auto* B : W.buckets) delete B;
   W.buckets.clear();
   if (!grouped) return;
@@ -665,7 +668,7 @@ static void fill_items(Plan& p, ClassPairWork& W, int force) {
   });
   for (auto& kv : by) {
     GenBucket* B = kv.second;
-    B->h_items = B->all_items;
+    B->h_items.clear();
     B->nwork = (int)B->all_items.size();
     upload_items(B->work, B->split, B->all_items);
     W.buckets.push_back(B);
@@ -686,14 +689,15 @@ static void apply_shard(Plan& p, ClassPairWork& W) {
     q = pq = 0;
     for (int64_t i = 0; i < n; ++i) {
       if (owner[i] != rank) continue;
-      mine.push_back(all[i]);
+      if (world > 1) mine.push_back(all[i]);
       q += (long long)(all[i].z - all[i].y) * qmul;
       pq += cost[i];
     }
-    h = mine;
-    nwork = (int)mine.size();
-    if (!mine.empty())  // the buffer holds the full list, so it is never reallocated
-      CUDA_OK(cudaMemcpy(work.ptr, mine.data(), mine.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    const std::vector<int4>& act = world > 1 ? mine : all;
+    nwork = (int)act.size();
+    if (!act.empty())  // the buffer holds the full list, so it is never reallocated
+      CUDA_OK(cudaMemcpy(work.ptr, act.data(), act.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    h = std::move(mine);  // empty when unsharded: the active items are then `all`
   };
   shard(W.all_items, W.item_cost, W.work, W.h_items, W.nwork, W.quartets, W.prim_quartets, 1);
   for (auto* B : W.buckets)
@@ -706,7 +710,7 @@ static void apply_shard(Plan& p, ClassPairWork& W) {
 struct GenEntry {
   int cls = 0, mol = 0, diag = 0, pair = -1, nco = 1, ppoff = 0, npp = 0;
   int ws[4] = {0, 0, 0, 0}, wsb[4] = {0, 0, 0, 0};
-  std::pair<int, int> pkey;
+  long long pkey = 0;  // parent pair: max parent id * nparent + min parent id
 };
 
 static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double cut, int device) {
@@ -816,9 +820,10 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
   // pair carrying its contraction combinations, so primitive quartets shared
   // by the combinations are evaluated once.  Entries with a single
   // combination are the expanded pairs themselves.
-  std::map<std::pair<int, int>, int> ws_pair_id;
-  for (int q = 0; q < p.npair; ++q)
-    ws_pair_id[{std::max(p.pair_info[q].x, p.pair_info[q].y), std::min(p.pair_info[q].x, p.pair_info[q].y)}] = q;
+  std::unordered_map<long long, int> ws_pair_id;  // key: max(ws) * nws + min(ws)
+  ws_pair_id.reserve(2 * (size_t)p.npair + 1);
+  auto ws_key = [&](int a, int b) { return (long long)std::max(a, b) * p.nws + std::min(a, b); };
+  for (int q = 0; q < p.npair; ++q) ws_pair_id[ws_key(p.pair_info[q].x, p.pair_info[q].y)] = q;
   std::vector<int> parent_ws0;  // first work shell of every parent shell
   for (int w = 0; w < p.nws; ++w)
     if (w == 0 || p.ws_parent[w] != p.ws_parent[w - 1]) parent_ws0.push_back(w);
@@ -838,11 +843,11 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
       base.cls = pair_class(std::max(la, lb), 0);
       base.mol = p.ws_info[parent_ws0[PA]].z;
       base.diag = PA == PB;
-      base.pkey = std::make_pair(std::max(p.ws_parent[parent_ws0[PA]], p.ws_parent[parent_ws0[PB]]),
-                                 std::min(p.ws_parent[parent_ws0[PA]], p.ws_parent[parent_ws0[PB]]));
+      base.pkey = (long long)std::max(p.ws_parent[parent_ws0[PA]], p.ws_parent[parent_ws0[PB]]) * parent_base[nmol] +
+                  std::min(p.ws_parent[parent_ws0[PA]], p.ws_parent[parent_ws0[PB]]);
       if (nca * ncb == 1) {
         int A = parent_ws0[PA], B = parent_ws0[PB];
-        auto it = ws_pair_id.find({std::max(A, B), std::min(A, B)});
+        auto it = ws_pair_id.find(ws_key(A, B));
         if (it == ws_pair_id.end()) continue;  // every primitive pair screened out
         base.pair = it->second;
         base.nco = 1;
@@ -990,11 +995,14 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
   std::vector<double> qw(p.npair);
   if (p.npair) CUDA_OK(cudaMemcpy(qw.data(), p.d_q_work.ptr, p.npair * sizeof(double), cudaMemcpyDeviceToHost));
   // parent-pair bound: max over the work pairs of the parent pair
-  std::map<std::pair<int, int>, double> parent;
+  // (parent key max * nparent + min)
+  const long long npar = (long long)parent_base[nmol];
+  std::unordered_map<long long, double> parent;
+  parent.reserve(2 * (size_t)p.npair + 1);
   auto pkey = [&](int q) {
     int a = p.ws_parent[p.pair_info[q].x], b = p.ws_parent[p.pair_info[q].y];
     if (a < b) std::swap(a, b);
-    return std::make_pair(a, b);
+    return (long long)a * npar + b;
   };
   for (int q = 0; q < p.npair; ++q) {
     auto k = pkey(q);
@@ -1070,19 +1078,22 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
   // the combinations of the grouped entries cover exactly the expanded
   // work pairs of their classes (checked once per plan, on the host)
   {
-    std::vector<std::set<std::pair<int, int>>> want(kPairClasses), got(kPairClasses);
+    std::vector<long long> want, got;  // (class, work-shell pair) keys
+    const long long span = (long long)p.nws * p.nws;
     for (int q = 0; q < p.npair; ++q) {
       const int c = p.pair_class[q];
-      if (c == 0 || c == 1 || c == 3 || c == 6)
-        want[c].insert({std::max(p.pair_info[q].x, p.pair_info[q].y), std::min(p.pair_info[q].x, p.pair_info[q].y)});
+      if (c == 0 || c == 1 || c == 3 || c == 6) want.push_back(c * span + ws_key(p.pair_info[q].x, p.pair_info[q].y));
     }
     for (const GenEntry& e : gen)
-      for (int k = 0; k < e.nco; ++k) got[e.cls].insert({std::max(e.ws[k], e.wsb[k]), std::min(e.ws[k], e.wsb[k])});
-    for (int c = 0; c < kPairClasses; ++c)
-      for (const auto& wp : want[c])
-        if (!got[c].count(wp))
-          throw Failure{B200JK_INTERNAL, "grouped pair list misses a work pair of class " + std::to_string(c)};
+      for (int k = 0; k < e.nco; ++k) got.push_back(e.cls * span + ws_key(e.ws[k], e.wsb[k]));
+    std::sort(want.begin(), want.end());
+    std::sort(got.begin(), got.end());
+    got.erase(std::unique(got.begin(), got.end()), got.end());
+    if (!std::includes(got.begin(), got.end(), want.begin(), want.end()))
+      throw Failure{B200JK_INTERNAL, "grouped pair list misses a work pair"};
   }
+  std::vector<double> gen_q(gen.size());
+  for (size_t i = 0; i < gen.size(); ++i) gen_q[i] = std::sqrt(parent[gen[i].pkey]);
   // ---- grouped lists: same screening and order, plus the number of
   // combinations (runs of equal (combinations, primitive pairs) per molecule)
   for (int c = 0; c < kPairClasses; ++c) {
@@ -1090,13 +1101,13 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     bool any_gen = false;
     for (size_t i = 0; i < gen.size(); ++i) {
       if (gen[i].cls != c) continue;
-      const double q = std::sqrt(parent[gen[i].pkey]);
+      const double q = gen_q[i];
       if (cut > 0 && q * qmax_mol[gen[i].mol] < cut) continue;
       ids.push_back((int)i);
       any_gen = any_gen || gen[i].nco > 1;
     }
     if (!any_gen) continue;  // identical to the expanded list
-    auto qof = [&](int i) { return std::sqrt(parent[gen[i].pkey]); };
+    auto qof = [&](int i) { return gen_q[i]; };
     std::sort(ids.begin(), ids.end(), [&](int a, int b) {
       const GenEntry &ea = gen[a], &eb = gen[b];
       if (ea.mol != eb.mol) return ea.mol < eb.mol;
@@ -1173,13 +1184,10 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     long long total = 0;
     std::vector<std::vector<double>> pq(nmol);
     // parent pair bounds per molecule
-    std::map<std::pair<int, int>, double> seen;
-    for (int q = 0; q < p.npair; ++q) seen[pkey(q)] = p.pair_q[q];
-    for (auto& kv : seen) {
-      int m = 0;
-      while (m + 1 < nmol + 1 && parent_base[m + 1] <= kv.first.first) ++m;
-      pq[m].push_back(kv.second);
-    }
+    std::unordered_map<long long, char> seen;
+    seen.reserve(2 * (size_t)p.npair + 1);
+    for (int q = 0; q < p.npair; ++q)
+      if (seen.emplace(pkey(q), 1).second) pq[p.ws_info[p.pair_info[q].x].z].push_back(p.pair_q[q]);
     for (int m = 0; m < nmol; ++m) {
       auto& v = pq[m];
       std::sort(v.begin(), v.end(), std::greater<double>());

@@ -52,7 +52,7 @@ struct ClassPairWork {
   DevBuf split;                 // int per work item: first FP32 ket (filled per call)
   long long quartets = 0;       // significant work-shell quartets in this class pair
   long long prim_quartets = 0;  // their primitive quartets
-  std::vector<int4> h_items;    // host copy of the active work items (this rank's shard)
+  std::vector<int4> h_items;    // this rank's items when the plan is sharded (empty: all_items)
   std::vector<int4> all_items;  // every work item of the class pair
   std::vector<int64_t> item_cost;  // primitive quartets per item (all_items order)
   // grouped lists (contraction combinations shared): the J/K work is in
