@@ -451,7 +451,10 @@ static void validate_tables(const b200jk_molecule& m, int cart) {
     invalid("Invalid libcint table dimensions or operator");
   for (int i = 0; i < m.nenv; ++i)
     if (!std::isfinite(m.env[i])) invalid("Native integral env must be finite");
-  if (m.env[8] != 0.0) throw Failure{B200JK_UNSUPPORTED, "Range-separated (omega != 0) J/K is not built on the B200 path"};
+  // env[8] (libcint PTR_RANGE_OMEGA): omega > 0 selects erf(omega r)/r, as the
+  // reference's long-range J/K sets it (plan.py:86-87); the short-range
+  // (omega < 0) operator is not built
+  if (m.env[8] < 0.0) throw Failure{B200JK_UNSUPPORTED, "Short-range (omega < 0) J/K is not built on the B200 path"};
   for (int a = 0; a < m.natm; ++a) {
     const int32_t* row = m.atm + a * 6;
     if (row[1] < 20 || row[1] + 3 > m.nenv || row[2] != 1)
@@ -548,6 +551,7 @@ static JKArgs base_args(const Plan& p) {
   a.pp_f = p.d_pp_f.as<float4>();
   a.pp_f2 = p.d_pp_f2.as<float2>();
   a.pp_c = p.d_pp_c.as<double4>();
+  a.omega2 = p.omega * p.omega;
   a.pp_cf = p.d_pp_cf.as<float4>();
   a.ws_atm = p.d_ws_atm.as<int>();
   a.mol_base = p.d_mol_base_cart.as<long long>();
@@ -723,6 +727,9 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
   Plan& p = *plan;
   p.device = device;
   p.cart = cart;
+  p.omega = mols[0].env[8];
+  for (int m = 1; m < nmol; ++m)
+    if (mols[m].env[8] != p.omega) invalid("All molecules of a batch need the same range parameter env[8]");
   p.cutoff = cut;
   p.nmol = nmol;
   // ---- work shells (one per contraction column of every shell)

@@ -41,6 +41,7 @@ struct JKArgs {
   const double4* pp_c;       // per primitive pair: coefficients of up to 4 combinations
   const float4* pp_cf;       // the same in FP32
   int same_list;
+  double omega2;             // long-range erf(omega r)/r operator: omega^2 (0: full Coulomb)
   const int4* work;          // (bra position, ket begin, ket end, unused)
   int nwork;
   const int* split;          // per work item: first ket computed in FP32
@@ -97,6 +98,7 @@ struct QuartetGeom {
   double abx, aby, abz, cdx, cdy, cdz;
   int aoA, aoB, aoC, aoD, mol;
   double scale;
+  double omega2;   // erf-attenuated operator: omega^2 (0: full Coulomb)
 };
 
 __device__ __forceinline__ void load_quartet(const JKArgs& args, int bra, int ket, QuartetGeom& g) {
@@ -118,6 +120,7 @@ __device__ __forceinline__ void load_quartet(const JKArgs& args, int bra, int ke
   if (g.C == g.D) s *= 0.5;
   if (bra == ket) s *= 0.5;
   g.scale = s;
+  g.omega2 = args.omega2;
 }
 
 // Bra side of a work item from the per-position records (loaded once per warp).
@@ -151,6 +154,7 @@ __device__ __forceinline__ void load_quartet_rec(const JKArgs& args, const BraRe
   if (kx.z == kx.w) s *= 0.5;
   if (args.same_list && kpos == b.pos) s *= 0.5;
   g.scale = s;
+  g.omega2 = args.omega2;
 }
 
 // Per primitive quartet scalars.
@@ -160,7 +164,24 @@ struct PrimQ {
   R inv2p, inv2q;            // 1/(2p), 1/(2q)
   R pax, pay, paz, qcx, qcy, qcz, pqx, pqy, pqz;
   R t, pref;
+  R theta;                   // omega^2 / (omega^2 + rho) for erf(omega r)/r, else 1
 };
+
+// erf(omega r)/r (libcint's PTR_RANGE_OMEGA > 0): with theta = omega^2 /
+// (omega^2 + pq/(p+q)) the Boys functions become theta^(m+1/2) F_m(theta T),
+// i.e. Rys roots at theta T, nodes t^2 scaled by theta (root_coef) and
+// weights by sqrt(theta) (folded into pref).
+template <typename R>
+__device__ __forceinline__ void apply_range(double omega2, R p, R q, R ipq, PrimQ<R>& s) {
+  s.theta = R(1);
+  if (omega2 > 0.0) {
+    const R w2 = R(omega2);
+    const R th = w2 / (w2 + p * q * ipq);
+    s.t *= th;
+    s.pref *= dsqrt<R>(th);
+    s.theta = th;
+  }
+}
 
 // Division-free: pref = 2 pi^2.5 (K_ab/p)(K_cd/q) / sqrt(p+q) with the
 // per-pair factors precomputed; 1/(p+q) = rsqrt(p+q)^2.
@@ -184,6 +205,7 @@ __device__ __forceinline__ void prim_setup(const QuartetGeom& g, const double4 P
     s.pax = float(P.x - g.ax); s.pay = float(P.y - g.ay); s.paz = float(P.z - g.az);
     s.qcx = float(Q.x - g.cx); s.qcy = float(Q.y - g.cy); s.qcz = float(Q.z - g.cz);
     s.pqx = pqx; s.pqy = pqy; s.pqz = pqz;
+    apply_range<R>(g.omega2, R(p), R(q), R(ipq), s);
     return;
   }
   const double p = P.w, q = Q.w;
@@ -202,12 +224,14 @@ __device__ __forceinline__ void prim_setup(const QuartetGeom& g, const double4 P
   s.pax = R(P.x - g.ax); s.pay = R(P.y - g.ay); s.paz = R(P.z - g.az);
   s.qcx = R(Q.x - g.cx); s.qcy = R(Q.y - g.cy); s.qcz = R(Q.z - g.cz);
   s.pqx = R(pqx); s.pqy = R(pqy); s.pqz = R(pqz);
+  apply_range<R>(g.omega2, R(p), R(q), R(ipq), s);
 }
 
 // FP32 quartets: per-primitive data stored relative to the shell centre in
 // FP32, P - Q = (A - C) + (P - A) - (Q - C) with A - C formed once per quartet.
 __device__ __forceinline__ void prim_setup_f(const float3 ac, const float4 P, const float2 PA,
-                                             const float4 Q, const float2 QA, PrimQ<float>& s) {
+                                             const float4 Q, const float2 QA, PrimQ<float>& s,
+                                             double omega2) {
   const float p = P.w, q = Q.w;
   const float pq = p + q;
   const float rs = rsqrtf(pq);
@@ -223,6 +247,7 @@ __device__ __forceinline__ void prim_setup_f(const float3 ac, const float4 P, co
   s.pax = P.x; s.pay = P.y; s.paz = P.z;
   s.qcx = Q.x; s.qcy = Q.y; s.qcz = Q.z;
   s.pqx = pqx; s.pqy = pqy; s.pqz = pqz;
+  apply_range<float>(omega2, p, q, ipq, s);
 }
 
 // Primitive-pair storage type per precision (bra cache and ket reads).
@@ -245,7 +270,7 @@ __device__ __forceinline__ void prim_any(const QuartetGeom& g, const float3 ac,
                                          const typename PrimData<R>::A P, const typename PrimData<R>::B PA,
                                          const typename PrimData<R>::A Q, const typename PrimData<R>::B QA,
                                          PrimQ<R>& s) {
-  if constexpr (sizeof(R) == 4) prim_setup_f(ac, P, PA, Q, QA, s);
+  if constexpr (sizeof(R) == 4) prim_setup_f(ac, P, PA, Q, QA, s, g.omega2);
   else prim_setup<double>(g, P, PA, Q, QA, s);
 }
 
@@ -257,7 +282,8 @@ struct RootCoef {
 };
 
 template <typename R>
-__device__ __forceinline__ void root_coef(const PrimQ<R>& s, R u, RootCoef<R>& rc) {
+__device__ __forceinline__ void root_coef(const PrimQ<R>& s, R u0, RootCoef<R>& rc) {
+  const R u = u0 * s.theta;  // node t^2 (scaled for the erf-attenuated operator)
   const R up = u * s.pq_inv;
   rc.b00 = R(0.5) * up;
   rc.b10 = s.inv2p - s.inv2p * u * s.q_pq;

@@ -96,6 +96,7 @@ struct Plan {
   int shard_rank = 0, shard_world = 1;  // active work-item shard
   int cart = 0;
   double cutoff = 0.0;
+  double omega = 0.0;   // env[8]: erf(omega r)/r operator when > 0
   int nmol = 0;
   // per molecule
   std::vector<int> mol_nout, mol_ncart, mol_natm, mol_atm_off;

@@ -289,15 +289,27 @@ class IntegralPlan:
 
     def get_jk(self, parameters, density, *, screening_threshold=0.0, workers=1, with_j=True,
                with_k=True, omega=0.0, precision="fp64", fp32_cut=DEFAULT_FP32_CUT):
-        if omega:
-            raise NotImplementedError("Range-separated (omega > 0) J/K is not built on the B200 path.")
+        omega = validate_omega(omega)
         atm, bas, env = self.pack(parameters)
+        if omega:
+            env = np.array(env, dtype=np.float64, copy=True)
+            env[8] = omega  # libcint PTR_RANGE_OMEGA: erf(omega r)/r (plan.py:86-87)
         d = torch.as_tensor(density)
         if d.shape[-2:] != (self.topology.nao,) * 2:
             raise ValueError("Density AO dimensions do not match the plan.")
         return direct_jk(atm, bas, env, density, cart=self.topology.cart, cutoff=screening_threshold,
                          workers=workers, with_j=with_j, with_k=with_k, precision=precision,
                          fp32_cut=fp32_cut)
+
+
+def validate_omega(omega):
+    """Static nonnegative erf-Coulomb range parameter in inverse Bohr (plan.py:18-27)."""
+    if isinstance(omega, (bool, np.bool_)) or not isinstance(omega, (int, float, np.integer, np.floating)):
+        raise TypeError("omega must be a static real scalar.")
+    omega = float(omega)
+    if not np.isfinite(omega) or omega < 0 or omega > np.sqrt(np.finfo(np.float64).max) / 2:
+        raise ValueError("omega must be finite, nonnegative and at most sqrt(float64.max)/2.")
+    return omega
 
 
 def make_plan(topology: BasisTopology) -> IntegralPlan:
@@ -320,3 +332,48 @@ class NativeDirectBasis:
         return self.plan.get_jk(self.parameters, density, screening_threshold=screening_threshold,
                                 workers=workers, with_j=with_j, with_k=with_k, omega=omega,
                                 precision=precision, fp32_cut=fp32_cut)
+
+    def prepare_jk(self, *, cache_bytes=0, screening_threshold=0.0, workers=1, with_j=True, with_k=True,
+                   omega=0.0, precision="fp64", fp32_cut=DEFAULT_FP32_CUT):
+        """Bind one response action: density batch -> (J, K) (backends/native/jk.py:118-162).
+
+        On CUDA arrays the reference's prepared action is the direct J/K
+        (its ``platform_dependent`` default branch); here too.  The device
+        plan for these tables is built on the first call and reused by every
+        later one, so batches of response densities cost one launch set each.
+        `cache_bytes` is accepted for signature compatibility; no ERIs are
+        stored.
+        """
+        omega = validate_omega(omega)
+
+        def action(density):
+            return self.get_jk(density, screening_threshold=screening_threshold, workers=workers,
+                               with_j=with_j, with_k=with_k, omega=omega, precision=precision,
+                               fp32_cut=fp32_cut)
+        return action
+
+
+def rsh_jk(provider, density, coefficients, *, with_j=True, with_k=True, screening_threshold=0.0,
+           workers=1, precision="fp64", fp32_cut=DEFAULT_FP32_CUT):
+    """Range-separated-hybrid J/K (scf/rsh.py:62-85): the full Coulomb J and
+    K_rsh = sr * K(full) + (lr - sr) * K(omega) for coefficients
+    (omega, long_range, short_range)."""
+    if len(coefficients) != 3:
+        raise ValueError("RSH J/K requires (omega, long_range, short_range) coefficients.")
+    omega, long_range, short_range = (float(v) for v in coefficients)
+    if not all(np.isfinite(v) for v in (omega, long_range, short_range)) or omega <= 0.0:
+        raise ValueError("RSH J/K requires finite coefficients and positive omega.")
+    d = torch.as_tensor(density)
+    coulomb = exchange = torch.zeros_like(d)
+    opts = dict(screening_threshold=screening_threshold, workers=workers, precision=precision, fp32_cut=fp32_cut)
+    if with_j or (with_k and short_range != 0.0):
+        coulomb, full_k = provider.get_jk(density, with_j=with_j, with_k=with_k and short_range != 0.0,
+                                          omega=0.0, **opts)
+        if with_k:
+            exchange = short_range * full_k
+    if with_k and long_range != short_range:
+        _, long_k = provider.get_jk(density, with_j=False, with_k=True, omega=omega, **opts)
+        exchange = exchange + (long_range - short_range) * long_k
+    if not with_j:
+        coulomb = torch.zeros_like(d)
+    return coulomb, exchange

@@ -191,3 +191,45 @@ def test_autotune_keeps_results():
     for p_ in ("fp64", "split"):
         got = plan.jk_packed(d, hermi=1, precision=p_)
         assert (got - ref[p_]).abs().max().item() < 1e-11
+
+
+@pytest.mark.parametrize("basis,cart", [("6-31g*", False), ("6-31g*", True), ("cc-pvdz", False)])
+def test_long_range_omega_vs_oracle(basis, cart):
+    # erf(omega r)/r integrals (libcint PTR_RANGE_OMEGA = env[8], as the
+    # reference's get_jk sets it, plan.py:86-87): FP64 J/K to 1e-10 of the
+    # oracle, screening bounds included; a nonsymmetric density as well
+    top, par, sa, atm, bas, env = tables(WATER, basis, cart)
+    env = np.array(env, dtype=np.float64, copy=True)
+    env[8] = 0.33
+    n = top.nao
+    rng = np.random.default_rng(17)
+    for d in (psd_density(n, 5, 3), rng.normal(size=(n, n))):
+        j0, k0 = oracle.direct_jk(atm, bas, env, d, cart=cart, cutoff=1e-12, workers=8)
+        j, k = J.direct_jk(atm, bas, env, torch.as_tensor(d, device="cuda"), cart=cart, cutoff=1e-12)
+        assert np.abs(j.cpu().numpy() - j0).max() < 1e-10
+        assert np.abs(k.cpu().numpy() - k0).max() < 1e-10
+    # the long-range integrals really differ from the Coulomb ones
+    jf, _ = oracle.direct_jk(atm, bas, np.where(np.arange(env.size) == 8, 0.0, env), d, cart=cart,
+                             cutoff=1e-12, workers=8)
+    assert np.abs(jf - j0).max() > 1e-2
+    js, ks = J.direct_jk(atm, bas, env, torch.as_tensor(psd_density(n, 5, 3), device="cuda"), cart=cart,
+                         cutoff=1e-12, precision="split")
+    j0, k0 = oracle.direct_jk(atm, bas, env, psd_density(n, 5, 3), cart=cart, cutoff=1e-12, workers=8)
+    assert np.abs(js.cpu().numpy() - j0).max() < 1e-6 and np.abs(ks.cpu().numpy() - k0).max() < 1e-6
+
+
+def test_prepare_jk_and_rsh_combination():
+    # prepare_jk (backends/native/jk.py:118-162) binds the direct action;
+    # rsh_jk = sr K(full) + (lr - sr) K(omega) with the full J (scf/rsh.py:62-85)
+    from gradscf_b200 import basis as B
+    top, par, sa = B.prepare_basis(WATER, "6-31g*", cart=False)
+    provider = J.NativeDirectBasis(J.make_plan(top), par)
+    d = torch.as_tensor(psd_density(top.nao, 5, 8), device="cuda")
+    act = provider.prepare_jk(omega=0.4)
+    jl, kl = act(d)
+    j2, k2 = provider.get_jk(d, omega=0.4)
+    assert (jl - j2).abs().max().item() < 1e-13 and (kl - k2).abs().max().item() < 1e-13
+    jf, kf = provider.get_jk(d)
+    jr, kr = J.rsh_jk(provider, d, (0.4, 0.65, 0.2))
+    assert (jr - jf).abs().max().item() < 1e-14
+    assert (kr - (0.2 * kf + 0.45 * kl)).abs().max().item() < 1e-12
