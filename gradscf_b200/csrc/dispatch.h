@@ -13,11 +13,13 @@ constexpr int kQuartetClasses = kPairClasses * (kPairClasses + 1) / 2;   // 55
 using JKLauncher = int (*)(const JKArgs&, cudaStream_t);
 using SchwarzLauncher = int (*)(const JKArgs&, int npairs, int cart, cudaStream_t);
 using GradLauncher = int (*)(const JKArgs&, cudaStream_t);
+using StoreLauncher = int (*)(const JKArgs&, int cart, int layout, double* out, long long npair, cudaStream_t);
 
 struct DispatchTable {
   JKLauncher jk64[kQuartetClasses] = {};
   JKLauncher jk32[kQuartetClasses] = {};
   GradLauncher grad64[kQuartetClasses] = {};
+  StoreLauncher store[kQuartetClasses] = {};   // packed ERI producer
   SchwarzLauncher schwarz[kPairClasses] = {};
   // grouped-list kernels by (bra, ket) combinations: slot 3*g(gb) + g(gk),
   // g(1) = 0, g(2) = 1, g(4) = 2 (slot 0 is the plain kernel above)

@@ -1783,6 +1783,32 @@ int b200jk_int1e_grad(b200jk_plan* plan, const double* d_density, const double* 
   });
 }
 
+int b200jk_packed_eri(b200jk_plan* plan, int32_t layout, double* d_out, int64_t out_size, void* stream) {
+  return guarded([&] {
+    if (!plan || !d_out) invalid("Invalid packed ERI request");
+    Plan& p = *plan->p;
+    if (p.nmol != 1) invalid("Packed ERIs are built for one-molecule plans");
+    if (layout != 0 && layout != 1) invalid("Packed ERI layout must be 0 (s4) or 1 (s8)");
+    const long long n = p.mol_nout[0], np = n * (n + 1) / 2;
+    const long long size = layout == 0 ? np * np : np * (np + 1) / 2;
+    if (out_size != size) invalid("Packed ERI shape mismatch");  // csrc/packed_eri.cc:7-9
+    CUDA_OK(cudaSetDevice(p.device));
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_OK(cudaMemsetAsync(d_out, 0, (size_t)size * sizeof(double), st));
+    JKArgs a = base_args(p);
+    const auto& disp = dispatch();
+    for (auto* W : p.work) {
+      if (W->nwork == 0) continue;
+      const int cls = quartet_class(W->x, W->y);
+      set_lists(a, p, *W);
+      a.work = W->work.as<int4>();
+      a.nwork = W->nwork;
+      const int rc = disp.store[cls](a, p.cart, layout, d_out, np, st);
+      if (rc) throw Failure{B200JK_INTERNAL, std::string("packed ERI launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+    }
+  });
+}
+
 int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_t nb,
                               const double* d_cot, int32_t with_j, int32_t with_k, double* d_grad,
                               void* stream) {

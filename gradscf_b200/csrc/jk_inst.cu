@@ -72,6 +72,28 @@ int launch_class(const JKArgs& args, cudaStream_t stream) {
   return (int)cudaGetLastError();
 }
 
+template <int LA, int LB, int LC, int LD>
+int launch_store(const JKArgs& args, int cart, int layout, double* out, long long npair, cudaStream_t stream) {
+  if (args.nwork <= 0) return 0;
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  constexpr int TEAM = Policy<LA, LB, LC, LD>::TEAM;
+  using SM = TeamSmem<LA, LB, LC, LD, double, TEAM>;
+  constexpr size_t per_team = SM::bytes() + (size_t)CI::NOUT * 8;
+  int teams = 128 / TEAM;
+  while (teams > 1 && per_team * teams > 200 * 1024) --teams;
+  const size_t smem = per_team * teams;
+  if (smem > 48 * 1024) {
+    static bool configured = false;
+    if (!configured) {
+      cudaFuncSetAttribute(eri_store_kernel<LA, LB, LC, LD, TEAM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      configured = true;
+    }
+  }
+  eri_store_kernel<LA, LB, LC, LD, TEAM><<<args.nwork, teams * TEAM, smem, stream>>>(args, cart, layout, out, npair);
+  return (int)cudaGetLastError();
+}
+
 template <int LA, int LB, int LC, int LD, typename R, int GB, int GK>
 int launch_gen(const JKArgs& args, cudaStream_t stream) {
   if (args.nwork <= 0) return 0;
@@ -157,6 +179,7 @@ void REG_NAME(BRA_CLASS, KET_CLASS)(DispatchTable& t) {
   t.jk64[id] = &launch_class<XA, XB, YA, YB, double>;
   t.jk32[id] = &launch_class<XA, XB, YA, YB, float>;
   t.grad64[id] = &launch_grad<XA, XB, YA, YB>;
+  t.store[id] = &launch_store<XA, XB, YA, YB>;
   t.reg_path[id] = Policy<XA, XB, YA, YB, float>::REG || Policy<XA, XB, YA, YB>::REG;
   t.tile[id] = Policy<XA, XB, YA, YB>::TILE;
   t.grouped[id] = GROUPED;

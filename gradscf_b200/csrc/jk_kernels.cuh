@@ -1178,3 +1178,101 @@ __global__ void schwarz_kernel(JKArgs args, int npairs, int cart) {
 }
 
 }  // namespace b200jk
+
+namespace b200jk {
+
+// ---------------------------------------------------------------------------
+// Packed ERI producer (the reference's packed_eri, csrc/packed_eri.cc): the
+// team path's contracted Cartesian block of one quartet, transformed index
+// by index to the output basis in shared memory and written to s4 (np x np)
+// or s8 (np(np+1)/2 pairs of pairs) storage, np = n(n+1)/2, pair(i,j) =
+// i(i+1)/2 + j for i >= j.  Every element of the block is written (equal
+// values at symmetric positions), so the shell quartets of the canonical
+// traversal cover the whole array.
+// ---------------------------------------------------------------------------
+// dst[..., f, ...] = sum_c src[..., c, ...] T[c][f] along `axis` of dims[4].
+__device__ __forceinline__ void transform_axis(const double* src, double* dst, const int* dims, int axis,
+                                               const double* T, int nf, int lane, int team) {
+  int od[4] = {dims[0], dims[1], dims[2], dims[3]};
+  od[axis] = nf;
+  const int total = od[0] * od[1] * od[2] * od[3];
+  int sstride = 1;
+  for (int x = 3; x > axis; --x) sstride *= dims[x];
+  for (int e = lane; e < total; e += team) {
+    int r = e, idx[4];
+    for (int x = 3; x >= 0; --x) {
+      idx[x] = r % od[x];
+      r /= od[x];
+    }
+    const int f = idx[axis];
+    idx[axis] = 0;
+    const int s0 = ((idx[0] * dims[1] + idx[1]) * dims[2] + idx[2]) * dims[3] + idx[3];
+    double acc = 0.0;
+    for (int c = 0; c < dims[axis]; ++c) {
+      const double t = T[c * kTW + f];
+      if (t != 0.0) acc += t * src[s0 + c * sstride];
+    }
+    dst[e] = acc;
+  }
+}
+
+__device__ __forceinline__ long long pair_idx(long long i, long long j) {
+  return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i;
+}
+
+template <int LA, int LB, int LC, int LD, int TEAM>
+__global__ void eri_store_kernel(JKArgs args, int cart, int layout, double* __restrict__ out, long long npair) {
+  using SM = TeamSmem<LA, LB, LC, LD, double, TEAM>;
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x % TEAM;
+  const int team = threadIdx.x / TEAM;
+  const int nteams = blockDim.x / TEAM;
+  const unsigned mask =
+      TEAM == 32 ? 0xffffffffu : (((1u << TEAM) - 1u) << ((threadIdx.x % 32) / TEAM * TEAM));
+  const size_t per_team = SM::bytes() + (size_t)CI::NOUT * 8;
+  unsigned char* mine = smem_raw + (size_t)team * per_team;
+  double* sm = reinterpret_cast<double*>(mine);
+  double* V = reinterpret_cast<double*>(mine + SM::vofs());
+  double* W = reinterpret_cast<double*>(mine + SM::bytes());  // second buffer of NOUT doubles
+  const int4 w = args.work[blockIdx.x];
+  const int bra = args.bra_pairs[w.x];
+  const int nf[4] = {cart ? CI::NA : 2 * LA + 1, cart ? CI::NB : 2 * LB + 1, cart ? CI::NC : 2 * LC + 1,
+                     cart ? CI::ND : 2 * LD + 1};
+  const double* T[4] = {args.tb.c2s + LA * kTS, args.tb.c2s + LB * kTS, args.tb.c2s + LC * kTS,
+                        args.tb.c2s + LD * kTS};
+  for (int k = w.y + team; k < w.z; k += nteams) {
+    QuartetGeom g;
+    load_quartet(args, bra, args.ket_pairs[k], g);
+    team_block<LA, LB, LC, LD, double, TEAM>(args, g, sm, V, lane, mask);
+    // V (Cartesian a,b,c,d) -> output basis, innermost index first
+    int dims[4] = {CI::NA, CI::NB, CI::NC, CI::ND};
+    double* src = V;
+    double* dst = W;
+    for (int axis = 3; axis >= 0; --axis) {
+      transform_axis(src, dst, dims, axis, T[axis], nf[axis], lane, TEAM);
+      __syncwarp(mask);
+      dims[axis] = nf[axis];
+      double* t = src;
+      src = dst;
+      dst = t;
+    }
+    const int o[4] = {args.sh_info[g.A].w, args.sh_info[g.B].w, args.sh_info[g.C].w, args.sh_info[g.D].w};
+    const int total = nf[0] * nf[1] * nf[2] * nf[3];
+    for (int e = lane; e < total; e += TEAM) {
+      const int fd = e % nf[3], fc = (e / nf[3]) % nf[2], fb = (e / (nf[3] * nf[2])) % nf[1];
+      const int fa = e / (nf[3] * nf[2] * nf[1]);
+      const long long ab = pair_idx(o[0] + fa, o[1] + fb), cd = pair_idx(o[2] + fc, o[3] + fd);
+      const double v = src[e];
+      if (layout == 0) {
+        out[ab * npair + cd] = v;
+        out[cd * npair + ab] = v;
+      } else {
+        out[pair_idx(ab, cd)] = v;
+      }
+    }
+    __syncwarp(mask);
+  }
+}
+
+}  // namespace b200jk

@@ -377,3 +377,57 @@ def rsh_jk(provider, density, coefficients, *, with_j=True, with_k=True, screeni
     if not with_j:
         coulomb = torch.zeros_like(d)
     return coulomb, exchange
+
+
+def packed_eri_shape(n, ndim):
+    """Shape of s8 (ndim 1) or s4 (ndim 2) packed ERIs of n AOs (molecular/jk.py)."""
+    np_ = n * (n + 1) // 2
+    return (np_ * (np_ + 1) // 2,) if ndim == 1 else (np_, np_)
+
+
+def packed_eri(atm, bas, env, *, cart, aosym="s8", cutoff=0.0, device=None):
+    """Exact packed ERIs on the GPU (the reference's plan.evaluate("eri", aosym=...)
+    through csrc/packed_eri.cc): aosym "s8" -> (np(np+1)/2,), "s4" -> (np, np)."""
+    if aosym not in ("s4", "s8"):
+        raise ValueError("aosym must be 's4' or 's8'")
+    plan = cached_plan(atm, bas, env, cart=cart, cutoff=cutoff, device=device)
+    n = plan.nao[0]
+    shape = packed_eri_shape(n, 1 if aosym == "s8" else 2)
+    out = torch.empty(shape, dtype=torch.float64, device=plan.device)
+    with torch.cuda.device(plan.device):
+        _capi.check(_capi.lib().b200jk_packed_eri(plan._h, 1 if aosym == "s8" else 0,
+                                                 ctypes.c_void_p(out.data_ptr()), out.numel(),
+                                                 _stream_handle()))
+    return out
+
+
+def packed_jk(eri, density, *, with_j=True, with_k=True):
+    """J/K from s8 or s4 packed ERIs (backends/native/jk.py packed_jk,
+    csrc/packed_jk.cc): (..., n, n) float64 or complex128 densities -> (J, K)."""
+    if not (with_j or with_k):
+        raise ValueError("Packed J/K requires at least one selected operator")
+    e = torch.as_tensor(eri)
+    d = torch.as_tensor(density, device=e.device)
+    n = d.shape[-1]
+    if e.dtype != torch.float64 or e.dim() not in (1, 2) or tuple(e.shape) != packed_eri_shape(n, e.dim()):
+        raise ValueError("Packed ERI/density shapes do not match.")
+    flat = d.reshape(-1, n, n)
+    count = flat.shape[0]
+    real = torch.cat((flat.real, flat.imag), 0) if d.is_complex() else flat
+    real = real.to(torch.float64).contiguous()
+    nops = int(bool(with_j)) + int(bool(with_k))
+    out = torch.empty((nops, real.shape[0], n, n), dtype=torch.float64, device=e.device)
+    with torch.cuda.device(e.device):
+        _capi.check(_capi.lib().b200jk_packed_jk(
+            ctypes.c_void_p(e.contiguous().data_ptr()), 1 if e.dim() == 1 else 0, e.numel(), n,
+            ctypes.c_void_p(real.data_ptr()), real.shape[0], ctypes.c_void_p(out.data_ptr()),
+            int(bool(with_j)), int(bool(with_k)), _stream_handle()))
+    if d.is_complex():
+        out = torch.complex(out[:, :count], out[:, count:])
+    out = out.reshape(nops, *d.shape)
+    return (out[0] if with_j else torch.zeros_like(d), out[-1] if with_k else torch.zeros_like(d))
+
+
+def build_jk_from_packed(eri, density):
+    """molecular/jk.py build_jk_from_packed: J and K from s4/s8 packed ERIs."""
+    return packed_jk(eri, density)

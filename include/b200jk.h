@@ -109,6 +109,22 @@ int b200jk_plan_split_stats(b200jk_plan* plan, void* stream, int64_t* q64, int64
 int b200jk_plan_set_profiling(b200jk_plan* plan, int32_t on);
 int b200jk_plan_profile(b200jk_plan* plan, double* ms64, double* ms32, int32_t* launches);
 
+/* Packed four-centre ERIs of a one-molecule plan (replaces packed_eri,
+ * csrc/packed_eri.cc:5-14): layout 0 = s4 (np x np), 1 = s8 (np(np+1)/2),
+ * np = n(n+1)/2 output AO pairs, pair(i,j) = i(i+1)/2 + j for i >= j.
+ * out_size must equal the layout's element count.  d_out is zeroed first;
+ * quartets below the plan's Schwarz cut stay zero (the reference uses
+ * cut 0 here). */
+int b200jk_packed_eri(b200jk_plan* plan, int32_t layout, double* d_out, int64_t out_size, void* stream);
+
+/* J/K from packed ERIs (replaces PackedJK, csrc/packed_jk.cc:6-80): d_eri in
+ * the s4 / s8 layout above (eri_size elements), nb real (n, n) densities
+ * (nonsymmetric allowed), d_out (with_j + with_k, nb, n, n) overwritten.
+ * No plan needed. */
+int b200jk_packed_jk(const double* d_eri, int32_t layout, int64_t eri_size, int32_t n,
+                     const double* d_density, int32_t nb, double* d_out, int32_t with_j,
+                     int32_t with_k, void* stream);
+
 /* Measured vector-pipe FMA throughput of the current device in TFLOP/s
  * (fp64 = 1: FP64, 0: FP32) -- the roofline denominator for the ERI kernels. */
 int b200jk_measure_fma_peak(int32_t fp64, double* tflops, void* stream);

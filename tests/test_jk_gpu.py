@@ -233,3 +233,37 @@ def test_prepare_jk_and_rsh_combination():
     jr, kr = J.rsh_jk(provider, d, (0.4, 0.65, 0.2))
     assert (jr - jf).abs().max().item() < 1e-14
     assert (kr - (0.2 * kf + 0.45 * kl)).abs().max().item() < 1e-12
+
+
+def _pack_s8(eri):
+    n = eri.shape[0]
+    i, j = np.tril_indices(n)
+    pairs = eri[i[:, None], j[:, None], i[None, :], j[None, :]]   # (np, np) s4
+    a, b = np.tril_indices(pairs.shape[0])
+    return pairs, pairs[a, b]
+
+
+@pytest.mark.parametrize("basis,cart", [("6-31g*", False), ("6-31g*", True), ("cc-pvdz", False)])
+def test_packed_eri_and_packed_jk_vs_oracle(basis, cart):
+    # producer: csrc/packed_eri.cc (cut 0, s4 and s8); consumer: csrc/packed_jk.cc
+    top, par, sa, atm, bas, env = tables(WATER, basis, cart)
+    eri = oracle.eri_s1(atm, bas, env, cart=cart)
+    s4_ref, s8_ref = _pack_s8(eri)
+    s8 = J.packed_eri(atm, bas, env, cart=cart, aosym="s8")
+    s4 = J.packed_eri(atm, bas, env, cart=cart, aosym="s4")
+    assert s8.shape == s8_ref.shape and s4.shape == s4_ref.shape
+    assert np.abs(s8.cpu().numpy() - s8_ref).max() < 1e-11
+    assert np.abs(s4.cpu().numpy() - s4_ref).max() < 1e-11
+    rng = np.random.default_rng(5)
+    d = rng.normal(size=(2, top.nao, top.nao))
+    jr, kr = oracle.full_jk(eri, d)
+    for packed in (s8, s4):
+        j, k = J.packed_jk(packed, torch.as_tensor(d, device="cuda"))
+        np.testing.assert_allclose(j.cpu().numpy(), jr, atol=1e-10)
+        np.testing.assert_allclose(k.cpu().numpy(), kr, atol=1e-10)
+    jc, kc = J.build_jk_from_packed(s8, torch.complex(torch.as_tensor(d[0], device="cuda"),
+                                                      torch.as_tensor(d[1], device="cuda")))
+    np.testing.assert_allclose(jc.real.cpu().numpy(), jr[0], atol=1e-10)
+    np.testing.assert_allclose(kc.imag.cpu().numpy(), kr[1], atol=1e-10)
+    with pytest.raises(ValueError):
+        J.packed_jk(s8[:-1], torch.as_tensor(d, device="cuda"))

@@ -42,9 +42,13 @@ def _vjp(plan, d, cot, with_j=True, with_k=True):
     return g.cpu().numpy()
 
 
-@pytest.mark.parametrize("basis,cart", [("6-31g*", False), ("6-31g*", True), ("cc-pvdz", False)])
-def test_geometry_vjp_vs_oracle_nonsymmetric(basis, cart):
+@pytest.mark.parametrize("basis,cart,omega", [("6-31g*", False, 0.0), ("6-31g*", True, 0.0),
+                                              ("cc-pvdz", False, 0.0), ("6-31g*", False, 0.33)])
+def test_geometry_vjp_vs_oracle_nonsymmetric(basis, cart, omega):
+    # omega > 0: the erf(omega r)/r derivative integrals (libcint env[8])
     top, par, sa, atm, bas, env = tables(WATER, basis, cart)
+    env = np.array(env, dtype=np.float64, copy=True)
+    env[8] = omega
     rng = np.random.default_rng(932)
     n = top.nao
     d = rng.normal(size=(2, n, n))
