@@ -152,13 +152,46 @@ def run_c4(nwater=64, seed=4, cycles=15, quick=False):
     return out
 
 
+def run_packed(nwater=4, seed=1, reps=5):
+    """Packed-ERI producer and consumer on (H2O)n cc-pVDZ: s8 ERIs of every
+    AO quartet (cut 0), then J/K of one density from them; the consumer
+    streams the s8 array once (HBM roofline: bytes read / time)."""
+    from . import basis as B
+    from . import jk as J
+    spec = W.water_cluster(nwater, seed)
+    top, par, _ = B.prepare_basis(spec, "cc-pvdz", cart=False)
+    atm, bas, env = B.pack(top, par)
+    n = top.nao
+    eri = J.packed_eri(atm, bas, env, cart=False, aosym="s8")
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(reps):
+        eri = J.packed_eri(atm, bas, env, cart=False, aosym="s8")
+    e1.record()
+    torch.cuda.synchronize()
+    t_eri = e0.elapsed_time(e1) / reps
+    d = torch.as_tensor(W.psd_density(n, 5 * nwater, 0), device=eri.device)
+    J.packed_jk(eri, d)
+    e0.record()
+    for _ in range(reps):
+        J.packed_jk(eri, d)
+    e1.record()
+    torch.cuda.synchronize()
+    t_jk = e0.elapsed_time(e1) / reps
+    nbytes = eri.numel() * 8
+    return {"config": "packed", "system": f"(H2O){nwater} cc-pVDZ", "nao": n, "s8_elements": eri.numel(),
+            "producer_ms": t_eri, "consumer_ms": t_jk,
+            "consumer_eri_read_gbs": nbytes / (t_jk * 1e-3) / 1e9}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("config", choices=("c0", "c2", "c3", "c4"))
+    ap.add_argument("config", choices=("c0", "c2", "c3", "c4", "packed"))
     ap.add_argument("--quick", action="store_true", help="reduced size (smoke run)")
     ap.add_argument("--cycles", type=int, default=15, help="c4: SCF iterations per precision")
     a = ap.parse_args(argv)
-    fn = {"c0": run_c0, "c2": run_c2, "c3": lambda: run_c3(quick=a.quick),
+    fn = {"c0": run_c0, "c2": run_c2, "c3": lambda: run_c3(quick=a.quick), "packed": run_packed,
           "c4": lambda: run_c4(cycles=a.cycles, quick=a.quick)}[a.config]
     if a.config == "c2" and a.quick:
         fn = lambda: run_c2(nwater=4)  # noqa: E731
