@@ -1212,6 +1212,11 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     }
     p.quartets = total;
   }
+  for (int i = 0; i < kAuxStreams; ++i) {
+    CUDA_OK(cudaStreamCreateWithFlags(&p.aux[i], cudaStreamNonBlocking));
+    CUDA_OK(cudaEventCreateWithFlags(&p.join_ev[i], cudaEventDisableTiming));
+  }
+  CUDA_OK(cudaEventCreateWithFlags(&p.fork_ev, cudaEventDisableTiming));
   return plan.release();
 }
 
@@ -1279,8 +1284,10 @@ static void split_units(Plan& p, ClassPairWork& W, double fp32_cut, cudaStream_t
 
 // The J/K kernels of class pair W (both slices in split mode), on the
 // densities and accumulators already set in `a`.
+// `only`: -1 launches every slice of `precision`; 1 only the FP64 slice and
+// 2 only the FP32 slice of a split build.
 static void launch_units(Plan& p, ClassPairWork& W, JKArgs a, int precision, cudaStream_t st,
-                         bool allow_profiling) {
+                         bool allow_profiling, int only = -1) {
   const auto& disp = dispatch();
   const int cls = quartet_class(W.x, W.y);
   for_each_unit(p, W, [&](const JKUnit& u) {
@@ -1311,10 +1318,49 @@ static void launch_units(Plan& p, ClassPairWork& W, JKArgs a, int precision, cud
     if (precision == B200JK_FP64) {
       launch(0, false);
     } else {
-      launch(1, false);
-      launch(2, true);
+      if (only != 2) launch(1, false);
+      if (only != 1) launch(2, true);
     }
   });
+}
+
+// Primitive quartets a class pair's J/K launches evaluate (scheduling weight).
+static long long jk_cost(const ClassPairWork& W) {
+  if (W.buckets.empty()) return W.prim_quartets;
+  long long c = 0;
+  for (const auto* B : W.buckets) c += B->prim_quartets;
+  return c;
+}
+
+// The class-pair launches of one build spread over the caller's stream and
+// the plan's auxiliary streams (forked from and joined back into `st`): the
+// launches are independent (J/K accumulate atomically), so their tails and
+// low-occupancy kernels overlap.  Longest-first onto the least-loaded
+// stream; in split builds the FP64 slices share one auxiliary stream.
+static void launch_all(Plan& p, JKArgs a, int precision, cudaStream_t st) {
+  CUDA_OK(cudaEventRecord(p.fork_ev, st));
+  for (int i = 0; i < kAuxStreams; ++i) CUDA_OK(cudaStreamWaitEvent(p.aux[i], p.fork_ev, 0));
+  cudaStream_t streams[kAuxStreams + 1] = {st};
+  for (int i = 0; i < kAuxStreams; ++i) streams[i + 1] = p.aux[i];
+  std::vector<std::pair<long long, ClassPairWork*>> order;
+  for (auto* W : p.work) order.push_back({jk_cost(*W), W});
+  std::sort(order.begin(), order.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+  const bool split = precision == B200JK_SPLIT;  // split builds: stream 1 carries the FP64 slices
+  std::vector<long long> load(kAuxStreams + 1, 0);
+  for (auto& [cost, W] : order) {
+    int best = -1;
+    for (int i = 0; i <= kAuxStreams; ++i) {
+      if (split && i == 1) continue;
+      if (best < 0 || load[i] < load[best]) best = i;
+    }
+    load[best] += cost;
+    launch_units(p, *W, a, precision, streams[best], false, split ? 2 : -1);
+    if (split) launch_units(p, *W, a, precision, streams[1], false, 1);
+  }
+  for (int i = 0; i < kAuxStreams; ++i) {
+    CUDA_OK(cudaEventRecord(p.join_ev[i], p.aux[i]));
+    CUDA_OK(cudaStreamWaitEvent(st, p.join_ev[i], 0));
+  }
 }
 
 // The J/K pipeline on caller-provided scratch: dens/dens_f hold (hermi ? nb :
@@ -1375,7 +1421,12 @@ void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j,
   a.nsym = nb;
   a.with_j = with_j;
   a.with_k = with_k;
-  for (auto* W : p.work) launch_units(p, *W, a, precision, st, allow_profiling);
+  if (p.profiling && allow_profiling) {
+    // serial, so that every class-pair launch is timed alone
+    for (auto* W : p.work) launch_units(p, *W, a, precision, st, true);
+  } else {
+    launch_all(p, a, precision, st);
+  }
   {
     const int no = max_no(p);
     const long long n2 = (long long)no * no;

@@ -91,8 +91,12 @@ struct ProfileEvent {
   cudaEvent_t start, stop;
 };
 
+constexpr int kAuxStreams = 3;  // streams besides the caller's for concurrent class-pair launches
+
 struct Plan {
   int device = 0;
+  cudaStream_t aux[kAuxStreams] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[kAuxStreams] = {};
   int shard_rank = 0, shard_world = 1;  // active work-item shard
   int cart = 0;
   double cutoff = 0.0;
@@ -142,6 +146,11 @@ struct Plan {
   bool profiling = false;
   std::vector<ProfileEvent> events;
   ~Plan() {
+    for (int i = 0; i < kAuxStreams; ++i) {
+      if (aux[i]) cudaStreamDestroy(aux[i]);
+      if (join_ev[i]) cudaEventDestroy(join_ev[i]);
+    }
+    if (fork_ev) cudaEventDestroy(fork_ev);
     for (auto* w : work) delete w;
     for (auto& e : events) {
       cudaEventDestroy(e.start);
