@@ -1894,8 +1894,26 @@ int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_
     a.gnb = nb;
     a.grad = d_grad;
     const auto& disp = dispatch();
-    for (auto* W : p.work) {
+    // class pairs longest-first over the caller's and the auxiliary streams
+    // (serial while profiling, so each launch is timed alone)
+    const int nstreams = p.profiling ? 1 : kAuxStreams + 1;
+    cudaStream_t streams[kAuxStreams + 1] = {st};
+    for (int i = 0; i < kAuxStreams; ++i) streams[i + 1] = p.aux[i];
+    if (nstreams > 1) {
+      CUDA_OK(cudaEventRecord(p.fork_ev, st));
+      for (int i = 0; i < kAuxStreams; ++i) CUDA_OK(cudaStreamWaitEvent(p.aux[i], p.fork_ev, 0));
+    }
+    std::vector<std::pair<long long, ClassPairWork*>> order;
+    for (auto* W : p.work) order.push_back({W->prim_quartets, W});
+    std::sort(order.begin(), order.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    std::vector<long long> load(nstreams, 0);
+    for (auto& [cost, W] : order) {
       if (W->nwork == 0) continue;
+      int best = 0;
+      for (int i = 1; i < nstreams; ++i)
+        if (load[i] < load[best]) best = i;
+      load[best] += cost;
+      cudaStream_t ls = streams[best];
       const int cls = quartet_class(W->x, W->y);
       set_lists(a, p, *W);
       a.work = W->work.as<int4>();
@@ -1905,15 +1923,20 @@ int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_
       if (p.profiling) {
         CUDA_OK(cudaEventCreate(&ev.start));
         CUDA_OK(cudaEventCreate(&ev.stop));
-        CUDA_OK(cudaEventRecord(ev.start, st));
+        CUDA_OK(cudaEventRecord(ev.start, ls));
       }
-      const int rc = disp.grad64[cls](a, st);
+      const int rc = disp.grad64[cls](a, ls);
       if (rc) throw Failure{B200JK_INTERNAL, std::string("gradient launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
       if (p.profiling) {
-        CUDA_OK(cudaEventRecord(ev.stop, st));
+        CUDA_OK(cudaEventRecord(ev.stop, ls));
         p.events.push_back(ev);
       }
     }
+    if (nstreams > 1)
+      for (int i = 0; i < kAuxStreams; ++i) {
+        CUDA_OK(cudaEventRecord(p.join_ev[i], p.aux[i]));
+        CUDA_OK(cudaStreamWaitEvent(st, p.join_ev[i], 0));
+      }
   });
 }
 

@@ -91,7 +91,10 @@ struct ProfileEvent {
   cudaEvent_t start, stop;
 };
 
-constexpr int kAuxStreams = 3;  // streams besides the caller's for concurrent class-pair launches
+#ifndef B200JK_AUX_STREAMS
+#define B200JK_AUX_STREAMS 3
+#endif
+constexpr int kAuxStreams = B200JK_AUX_STREAMS;  // streams besides the caller's for concurrent class-pair launches
 
 struct Plan {
   int device = 0;
