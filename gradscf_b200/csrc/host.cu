@@ -1706,6 +1706,25 @@ int b200jk_plan_autotune(b200jk_plan* plan, const double* d_density, int32_t nb,
   });
 }
 
+int b200jk_plan_launches(const b200jk_plan* plan, int32_t precision, int64_t* count) {
+  return guarded([&] {
+    if (!plan || !count) invalid("Invalid plan query");
+    const Plan& p = *plan->p;
+    long long units = 0, lists = 0;
+    for (auto* W : p.work) {
+      if (!W->buckets.empty()) {
+        for (auto* B : W->buckets) units += B->nwork > 0;
+      } else {
+        units += W->nwork > 0;
+      }
+    }
+    for (int c = 0; c < kPairClasses; ++c) lists += !p.classes[c].q.empty() + !p.grouped[c].q.empty();
+    // density_in + jk_out; split: to_float, maxabs, rowmax, one row-max pass
+    // per list, one boundary kernel and two J/K slices per unit
+    *count = precision == B200JK_SPLIT ? 2 + 3 + lists + 3 * units : 2 + units;
+  });
+}
+
 int b200jk_plan_set_shard(b200jk_plan* plan, int32_t rank, int32_t world) {
   return guarded([&] {
     if (!plan) invalid("Invalid plan");

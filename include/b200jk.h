@@ -125,6 +125,10 @@ int b200jk_packed_jk(const double* d_eri, int32_t layout, int64_t eri_size, int3
                      const double* d_density, int32_t nb, double* d_out, int32_t with_j,
                      int32_t with_k, void* stream);
 
+/* Number of kernels one b200jk_direct_jk call launches on this plan (and
+ * shard) in `precision` mode. */
+int b200jk_plan_launches(const b200jk_plan* plan, int32_t precision, int64_t* count);
+
 /* Measured vector-pipe FMA throughput of the current device in TFLOP/s
  * (fp64 = 1: FP64, 0: FP32) -- the roofline denominator for the ERI kernels. */
 int b200jk_measure_fma_peak(int32_t fp64, double* tflops, void* stream);
