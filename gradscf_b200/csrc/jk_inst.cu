@@ -29,8 +29,16 @@ struct Policy {
   // run 3-6x faster there than on the tile path)
   static constexpr int LIMIT = sizeof(R) == 4 ? B200JK_REG_LIMIT32 : 96;
   static constexpr bool REG = (3 * CI::NG + CI::NOUT <= LIMIT) && CI::NROOT <= 3;
-  // tile path: kets up to d x d (NCD <= 36), bra pair fits one block
-  static constexpr bool TILE = !REG && CI::NCD <= 36 && CI::NAB <= 128;
+  // tile path: kets up to d x d (NCD <= 36), bra pair fits one block; FP32
+  // accumulators take half the registers, so FP32 takes kets up to f x s / d x p
+#ifndef B200JK_TILE_NCD32
+#define B200JK_TILE_NCD32 100   // measured on (H2O)8 cc-pVTZ: split kernels 92.5 -> 84.8 ms
+#endif
+#ifndef B200JK_TILE_NCD64
+#define B200JK_TILE_NCD64 100  // measured on (H2O)8 cc-pVTZ: FP64 kernels 102.0 -> 91.4 ms (despite spills)
+#endif
+  static constexpr int TILE_NCD = sizeof(R) == 4 ? B200JK_TILE_NCD32 : B200JK_TILE_NCD64;
+  static constexpr bool TILE = !REG && CI::NCD <= TILE_NCD && CI::NAB <= 128;
   static constexpr int TEAM = CI::NOUT <= 4 * 24 ? 4 : CI::NOUT <= 8 * 24 ? 8 : CI::NOUT <= 16 * 24 ? 16 : 32;
 };
 

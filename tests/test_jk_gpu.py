@@ -267,3 +267,18 @@ def test_packed_eri_and_packed_jk_vs_oracle(basis, cart):
     np.testing.assert_allclose(kc.imag.cpu().numpy(), kr[1], atol=1e-10)
     with pytest.raises(ValueError):
         J.packed_jk(s8[:-1], torch.as_tensor(d, device="cuda"))
+
+
+def test_split_cc_pvtz_high_l_classes():
+    # f shells on O, d on H: the FP32 tile path for kets up to f x f in split mode
+    atom = "O 0 0 0; H 0 0.7572 0.5865; H 0 -0.7572 0.5865; O 2.9 0.1 0; H 3.5 0.8 0.3; H 3.4 -0.7 0.2"
+    top, par, sa, atm, bas, env = tables(atom, "cc-pvtz", False)
+    d = psd_density(top.nao, 10, 2)
+    j0, k0 = oracle.direct_jk(atm, bas, env, d, cart=False, cutoff=1e-12, workers=8)
+    plan = J.DirectJKPlan([(atm, bas, env)], cart=False, cutoff=1e-12)
+    dd = torch.as_tensor(d, device="cuda").reshape(1, -1)
+    for precision, tol in (("fp64", 1e-10), ("split", 1e-6)):
+        out = plan.jk_packed(dd, hermi=1, precision=precision)
+        n = top.nao
+        assert np.abs(out[0, 0].reshape(n, n).cpu().numpy() - j0).max() < tol
+        assert np.abs(out[1, 0].reshape(n, n).cpu().numpy() - k0).max() < tol
