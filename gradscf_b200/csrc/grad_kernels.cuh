@@ -160,3 +160,126 @@ __global__ void grad_team_kernel(JKArgs args) {
 }
 
 }  // namespace b200jk
+
+namespace b200jk {
+
+// Register-path coordinate VJP for small classes: one lane per ket of a
+// work item (warp-granular items as the J/K register path), the raised 2D
+// integrals of one root in registers, nine derivative partials per lane;
+// the bra-centre partials (A, B fixed per warp) are warp-reduced.
+template <int LA, int LB, int LC, int LD>
+struct GradReg {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  static constexpr int NGR = (LA + 2) * (LB + 2) * (LC + 2) * (LD + 1);
+  static constexpr bool OK = 3 * NGR + CI::NOUT <= 64;
+};
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128, 3) grad_reg_kernel(JKArgs args) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using GC = GradCfg<LA, LB, LC, LD, 1>;
+  using GI = GIdx<LA + 1, LB + 1, LC + 1, LD>;
+  constexpr int N = GC::NROOT;
+  constexpr int NGR = GradReg<LA, LB, LC, LD>::NGR;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.x * 4 + warp;
+  if (item >= args.nwork) return;
+  const int4 w = args.work[item];
+  const int bra = args.bra_pairs[w.x];
+  double bA[3] = {0, 0, 0}, bB[3] = {0, 0, 0};
+  int atA = 0, atB = 0;
+  for (int k0 = w.y; k0 < w.z; k0 += 32) {
+    const bool active = k0 + lane < w.z;
+    const int k = active ? k0 + lane : w.z - 1;
+    QuartetGeom g;
+    load_quartet(args, bra, args.ket_pairs[k], g);
+    atA = args.ws_atm[g.A];
+    atB = args.ws_atm[g.B];
+    const long long base = args.mol_base[g.mol];
+    const int n = args.mol_n[g.mol];
+    double gam[CI::NOUT];
+    static_for<0, CI::NOUT>([&](auto O) {
+      constexpr int o = decltype(O)::value;
+      constexpr int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
+      constexpr int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
+      gam[o] = active ? g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id) : 0.0;
+    });
+    double dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
+    for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
+      const double4 P = args.pp_data[i];
+      const double2 PA = args.pp_aux[i];
+      const double alpha = args.pp_exp[i].x, beta = args.pp_exp[i].y;
+      for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
+        PrimQ<double> s;
+        prim_setup<double>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
+        const double gamma_c = args.pp_exp[j].x;
+        double x[N], wt[N];
+        rys_roots<N, double>(s.t, x, wt, args.tb);
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+          RootCoef<double> rc;
+          root_coef<double>(s, x[r], rc);
+          double G[3][NGR];
+          build_g<LA + 1, LB + 1, LC + 1, LD, double>(rc.c00[0], rc.c0p[0], rc.b10, rc.b01, rc.b00, 1.0, g.abx,
+                                                      g.cdx, G[0]);
+          build_g<LA + 1, LB + 1, LC + 1, LD, double>(rc.c00[1], rc.c0p[1], rc.b10, rc.b01, rc.b00, 1.0, g.aby,
+                                                      g.cdy, G[1]);
+          build_g<LA + 1, LB + 1, LC + 1, LD, double>(rc.c00[2], rc.c0p[2], rc.b10, rc.b01, rc.b00,
+                                                      wt[r] * s.pref, g.abz, g.cdz, G[2]);
+          static_for<0, CI::NOUT>([&](auto O) {
+            constexpr int o = decltype(O)::value;
+            constexpr int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
+            constexpr int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
+            double v[3], fa[3], fb[3], fc[3];
+            static_for<0, 3>([&](auto X) {
+              constexpr int ax = decltype(X)::value;
+              constexpr int a = ax == 0 ? cart_lx(LA, ia) : ax == 1 ? cart_ly(LA, ia) : cart_lz(LA, ia);
+              constexpr int b = ax == 0 ? cart_lx(LB, ib) : ax == 1 ? cart_ly(LB, ib) : cart_lz(LB, ib);
+              constexpr int c = ax == 0 ? cart_lx(LC, ic) : ax == 1 ? cart_ly(LC, ic) : cart_lz(LC, ic);
+              constexpr int d = ax == 0 ? cart_lx(LD, id) : ax == 1 ? cart_ly(LD, id) : cart_lz(LD, id);
+              v[ax] = G[ax][GI::idx(a, b, c, d)];
+              fa[ax] = 2.0 * alpha * G[ax][GI::idx(a + 1, b, c, d)];
+              fb[ax] = 2.0 * beta * G[ax][GI::idx(a, b + 1, c, d)];
+              fc[ax] = 2.0 * gamma_c * G[ax][GI::idx(a, b, c + 1, d)];
+              if constexpr (a > 0) fa[ax] -= a * G[ax][GI::idx(a - 1, b, c, d)];
+              if constexpr (b > 0) fb[ax] -= b * G[ax][GI::idx(a, b - 1, c, d)];
+              if constexpr (c > 0) fc[ax] -= c * G[ax][GI::idx(a, b, c - 1, d)];
+            });
+            const double gq = gam[o];
+            const double yz = v[1] * v[2], xz = v[0] * v[2], xy = v[0] * v[1];
+            dA[0] += gq * fa[0] * yz; dA[1] += gq * fa[1] * xz; dA[2] += gq * fa[2] * xy;
+            dB[0] += gq * fb[0] * yz; dB[1] += gq * fb[1] * xz; dB[2] += gq * fb[2] * xy;
+            dC[0] += gq * fc[0] * yz; dC[1] += gq * fc[1] * xz; dC[2] += gq * fc[2] * xy;
+          });
+        }
+      }
+    }
+    if (active) {
+      double* gC = args.grad + 3LL * args.ws_atm[g.C];
+      double* gD = args.grad + 3LL * args.ws_atm[g.D];
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        atomicAdd(gC + x, dC[x]);
+        atomicAdd(gD + x, -(dA[x] + dB[x] + dC[x]));
+        bA[x] += dA[x];
+        bB[x] += dB[x];
+      }
+    }
+  }
+#pragma unroll
+  for (int x = 0; x < 3; ++x)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      bA[x] += __shfl_down_sync(0xffffffffu, bA[x], off);
+      bB[x] += __shfl_down_sync(0xffffffffu, bB[x], off);
+    }
+  if (lane == 0) {
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      atomicAdd(args.grad + 3LL * atA + x, bA[x]);
+      atomicAdd(args.grad + 3LL * atB + x, bB[x]);
+    }
+  }
+}
+
+}  // namespace b200jk

@@ -137,6 +137,10 @@ int launch_schwarz(const JKArgs& args, int npairs, int cart, cudaStream_t stream
 template <int LA, int LB, int LC, int LD>
 int launch_grad(const JKArgs& args, cudaStream_t stream) {
   if (args.nwork <= 0) return 0;
+  if constexpr (GradReg<LA, LB, LC, LD>::OK) {
+    grad_reg_kernel<LA, LB, LC, LD><<<(args.nwork + 3) / 4, 128, 0, stream>>>(args);
+    return (int)cudaGetLastError();
+  }
   using CI = ClassInfo<LA, LB, LC, LD>;
   constexpr int TEAM = CI::NOUT <= 8 ? 4 : CI::NOUT <= 64 ? 8 : CI::NOUT <= 256 ? 16 : 32;
   using GC = GradCfg<LA, LB, LC, LD, TEAM>;
