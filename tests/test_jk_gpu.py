@@ -282,3 +282,50 @@ def test_split_cc_pvtz_high_l_classes():
         n = top.nao
         assert np.abs(out[0, 0].reshape(n, n).cpu().numpy() - j0).max() < tol
         assert np.abs(out[1, 0].reshape(n, n).cpu().numpy() - k0).max() < tol
+
+
+def test_simultaneous_calls_on_two_plans_keep_workspaces_separate():
+    # tests/integrals/test_native_direct_parallel.py:73-88: two plans, two
+    # host threads, each on its own stream; every result matches its oracle
+    from concurrent.futures import ThreadPoolExecutor
+    specs = (WATER, "H 0 0 0; H -0.2 0.3 1.8")
+    ctx = []
+    for atom in specs:
+        top, par, sa, atm, bas, env = tables(atom, "6-31g*", False)
+        plan = J.DirectJKPlan([(atm, bas, env)], cart=False, cutoff=1e-12)
+        d = np.random.default_rng(805).normal(size=(4, top.nao, top.nao))
+        ctx.append((plan, atm, bas, env, d))
+
+    def run(c, scale):
+        plan, atm, bas, env, d = c
+        stream = torch.cuda.Stream()
+        with torch.cuda.stream(stream):
+            dd = torch.as_tensor(scale * d, device="cuda").reshape(4, -1)
+            out = plan.jk_packed(dd, hermi=0, stream=stream)
+            stream.synchronize()
+            return out.cpu().numpy()
+
+    for c in ctx:
+        run(c, 1.0)  # plans and scratch initialised before the concurrent calls
+    with ThreadPoolExecutor(max_workers=2) as ex:
+        for scale in (1.0, 0.37):
+            futs = [ex.submit(run, c, scale) for c in ctx]
+            for f, (plan, atm, bas, env, d) in zip(futs, ctx):
+                got = f.result()
+                n = d.shape[-1]
+                j0, k0 = oracle.direct_jk(atm, bas, env, scale * d, cart=False, cutoff=1e-12, workers=4)
+                np.testing.assert_allclose(got[0].reshape(4, n, n), j0, atol=2e-10, rtol=1e-10)
+                np.testing.assert_allclose(got[1].reshape(4, n, n), k0, atol=2e-10, rtol=1e-10)
+
+
+def test_repeated_builds_agree_to_rounding():
+    # the reference's fixed-worker reduction is bitwise reproducible
+    # (test_native_direct_parallel.py:63-70); here J/K accumulate with
+    # atomics on the GPU, so repeats agree to rounding, not bit for bit
+    top, par, sa, atm, bas, env = tables(WATER, "cc-pvdz", False)
+    plan = J.DirectJKPlan([(atm, bas, env)], cart=False, cutoff=1e-12)
+    d = torch.as_tensor(np.random.default_rng(802).normal(size=(4, top.nao * top.nao)), device="cuda")
+    first = plan.jk_packed(d, hermi=0).clone()
+    for _ in range(3):
+        again = plan.jk_packed(d, hermi=0)
+        assert (again - first).abs().max().item() <= 1e-12 * max(1.0, first.abs().max().item())
