@@ -43,7 +43,8 @@ def _vjp(plan, d, cot, with_j=True, with_k=True):
 
 
 @pytest.mark.parametrize("basis,cart,omega", [("6-31g*", False, 0.0), ("6-31g*", True, 0.0),
-                                              ("cc-pvdz", False, 0.0), ("6-31g*", False, 0.33)])
+                                              ("cc-pvdz", False, 0.0), ("6-31g*", False, 0.33),
+                                              ("cc-pvtz", False, 0.0)])
 def test_geometry_vjp_vs_oracle_nonsymmetric(basis, cart, omega):
     # omega > 0: the erf(omega r)/r derivative integrals (libcint env[8])
     top, par, sa, atm, bas, env = tables(WATER, basis, cart)
