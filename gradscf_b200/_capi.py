@@ -23,6 +23,7 @@ EXPORTS = (
     "b200jk_direct_jk_noalloc", "b200jk_graph_create", "b200jk_graph_launch", "b200jk_graph_destroy",
     "b200jk_partition_items", "b200jk_plan_set_shard", "b200jk_plan_autotune",
     "b200jk_packed_eri", "b200jk_packed_jk", "b200jk_plan_launches",
+    "b200jk_direct_jk_geom_jvp", "b200jk_direct_jk_geom_hvp",
 )
 NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024
 NCLASS = 55
@@ -72,6 +73,8 @@ def lib():
     h.b200jk_direct_jk_tables.argtypes = [vp, i32, vp, i32, vp, i32, vp, i32, i32, vp, i32, f64,
                                           i32, i32, i32, vp]
     h.b200jk_direct_jk_geom_vjp.argtypes = [vp, vp, i32, vp, i32, i32, vp, vp]
+    h.b200jk_direct_jk_geom_jvp.argtypes = [vp, vp, i32, i32, vp, vp, i32, i32, vp, vp]
+    h.b200jk_direct_jk_geom_hvp.argtypes = [vp, vp, i32, vp, vp, i32, i32, vp, vp]
     h.b200jk_int1e.argtypes = [vp, i32, vp, vp]
     h.b200jk_int1e_grad.argtypes = [vp, vp, vp, vp, vp]
     p64 = ctypes.POINTER(i64)

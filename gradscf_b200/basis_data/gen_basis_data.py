@@ -2,7 +2,9 @@
 
 Run in a checkout that has the reference next to it:
 
-    python gradscf_b200/basis_data/gen_basis_data.py /root/reference
+    python gradscf_b200/basis_data/gen_basis_data.py <reference checkout>
+
+(or set GRADSCF_REFERENCE to the checkout and give no argument).
 
 It loads the reference's own snapshot parser
 (src/gradscf/integrals/basis/data/__init__.py, functions
@@ -41,4 +43,8 @@ def main(reference_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GRADSCF_REFERENCE")
+    if not root:
+        sys.exit("give the reference checkout as the argument or in GRADSCF_REFERENCE")
+    main(root)

@@ -78,13 +78,39 @@ def build(jobs=None, force=False, verbose=False):
     return LIB
 
 
+FFI_SRC = PKG / "ffi" / "b200jk_xla_ffi.cc"
+FFI_LIB = PKG / "_lib" / "libgradscf_b200_ffi.so"
+
+
+def build_ffi():
+    """The XLA FFI handler (ffi/b200jk_xla_ffi.cc), built only where JAX's FFI
+    headers exist (jax.ffi.include_dir()); returns the library path or None."""
+    try:
+        import jax  # noqa: F401
+        inc = jax.ffi.include_dir()
+    except Exception as e:  # JAX absent: the handler cannot be compiled
+        print(f"XLA FFI handler not built: {e}")
+        return None
+    lib = build()
+    cmd = [nvcc(), "-std=c++17", "-O2", "-Xcompiler", "-fPIC", "-shared", "-I", inc, "-I", str(INCLUDE),
+           str(FFI_SRC), "-o", str(FFI_LIB), "-L", str(lib.parent), "-lb200jk", "-Xlinker", "-rpath=$ORIGIN",
+           "-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"FFI handler build failed:\n{r.stderr[-4000:]}")
+    return FFI_LIB
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("-j", "--jobs", type=int, default=None)
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--ffi", action="store_true", help="also build the XLA FFI handler (needs JAX)")
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args(argv)
     print(build(a.jobs, a.force, a.verbose))
+    if a.ffi:
+        print(build_ffi())
 
 
 if __name__ == "__main__":

@@ -12,6 +12,8 @@ c3  256 water clusters, N ~ U{1..24} (seed 3), cluster m from seed 1000+m,
     per-cluster energy difference.
 c4  (H2O)64 cc-pVTZ (3712 functions, seed 4): J/K builds in FP64 and split
     mode along an RHF SCF (fragment guess, 15 iterations) and one force.
+prof  one small run of a kernel family for profiler captures (--case jk |
+    grad | packed, --nwater, --basis).
 Geometry generator and seeds: gradscf_b200/workloads.py.
 """
 from __future__ import annotations
@@ -185,14 +187,58 @@ def run_packed(nwater=4, seed=1, reps=5):
             "consumer_eri_read_gbs": nbytes / (t_jk * 1e-3) / 1e9}
 
 
+def run_prof(case="jk", nwater=8, basis="cc-pvdz", seed=1):
+    """One small run of a kernel family for profiler captures: `jk` one FP64
+    and one split J/K build of (H2O)n (seeded PSD density), `grad` one
+    coordinate VJP after them, `packed` the s8 producer and the consumer."""
+    from . import basis as B
+    from . import jk as J
+    spec = W.water_cluster(nwater, seed)
+    if case == "packed":
+        return run_packed(nwater=nwater, seed=seed, reps=1)
+    top, par, _ = B.prepare_basis(spec, basis, cart=False)
+    atm, bas, env = B.pack(top, par)
+    n = top.nao
+    plan = J.DirectJKPlan([(atm, bas, env)], cart=False, cutoff=1e-12)
+    d = torch.as_tensor(W.psd_density(n, 5 * nwater, 0), device=plan.device).reshape(1, -1)
+    out = {"config": "prof", "case": case, "system": f"(H2O){nwater} {basis}", "nao": n}
+    for precision in ("fp64", "split"):
+        e0, e1 = _events()
+        e0.record()
+        plan.jk_packed(d, hermi=1, precision=precision)
+        e1.record()
+        torch.cuda.synchronize()
+        out[f"{precision}_ms"] = e0.elapsed_time(e1)
+    if case == "grad":
+        import ctypes
+        from . import _capi
+        g = torch.zeros((plan.natm[0], 3), dtype=torch.float64, device=plan.device)
+        cot = torch.stack([d / 2.0, -d / 4.0]).contiguous()
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        e0, e1 = _events()
+        e0.record()
+        _capi.check(_capi.lib().b200jk_direct_jk_geom_vjp(plan._h, ctypes.c_void_p(d.data_ptr()), 1,
+                                                          ctypes.c_void_p(cot.data_ptr()), 1, 1,
+                                                          ctypes.c_void_p(g.data_ptr()), st))
+        e1.record()
+        torch.cuda.synchronize()
+        out["vjp_ms"] = e0.elapsed_time(e1)
+    plan.close()
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("config", choices=("c0", "c2", "c3", "c4", "packed"))
+    ap.add_argument("config", choices=("c0", "c2", "c3", "c4", "packed", "prof"))
     ap.add_argument("--quick", action="store_true", help="reduced size (smoke run)")
     ap.add_argument("--cycles", type=int, default=15, help="c4: SCF iterations per precision")
+    ap.add_argument("--case", default="jk", choices=("jk", "grad", "packed"), help="prof: kernel family")
+    ap.add_argument("--nwater", type=int, default=8, help="prof: cluster size")
+    ap.add_argument("--basis", default="cc-pvdz", help="prof: basis set")
     a = ap.parse_args(argv)
     fn = {"c0": run_c0, "c2": run_c2, "c3": lambda: run_c3(quick=a.quick), "packed": run_packed,
-          "c4": lambda: run_c4(cycles=a.cycles, quick=a.quick)}[a.config]
+          "c4": lambda: run_c4(cycles=a.cycles, quick=a.quick),
+          "prof": lambda: run_prof(a.case, a.nwater, a.basis)}[a.config]
     if a.config == "c2" and a.quick:
         fn = lambda: run_c2(nwater=4)  # noqa: E731
     print(json.dumps(fn()))

@@ -2,6 +2,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <cstdint>
+
 namespace b200jk {
 
 struct JKArgs;
@@ -18,6 +21,8 @@ using StoreLauncher = int (*)(const JKArgs&, int cart, int layout, double* out, 
 struct DispatchTable {
   JKLauncher jk64[kQuartetClasses] = {};
   JKLauncher jk32[kQuartetClasses] = {};
+  JKLauncher grp64[kQuartetClasses] = {};   // register path over bra groups (null: not built)
+  JKLauncher grp32[kQuartetClasses] = {};
   GradLauncher grad64[kQuartetClasses] = {};
   StoreLauncher store[kQuartetClasses] = {};   // packed ERI producer
   SchwarzLauncher schwarz[kPairClasses] = {};
@@ -25,6 +30,9 @@ struct DispatchTable {
   // g(1) = 0, g(2) = 1, g(4) = 2 (slot 0 is the plain kernel above)
   JKLauncher jkg64[kQuartetClasses][9] = {};
   JKLauncher jkg32[kQuartetClasses][9] = {};
+  // the same buckets on the bra-group register path (null: not built)
+  JKLauncher grpg64[kQuartetClasses][9] = {};
+  JKLauncher grpg32[kQuartetClasses][9] = {};
   bool grouped[kQuartetClasses] = {};    // the class pair takes grouped lists
   bool reg_path[kQuartetClasses] = {};   // either precision runs the register path
   bool tile[kQuartetClasses] = {};       // the FP64 kernel is the tile path
@@ -95,5 +103,19 @@ B200JK_FOR_EACH_CLASS_PAIR(B200JK_DECLARE_REG)
 #undef B200JK_DECLARE_REG
 
 const DispatchTable& dispatch();
+
+// Dynamic shared memory above 48 KB is an opt-in attribute of each kernel in
+// each device's context: set it on the current device the first time a
+// kernel is launched there (bit d of `done` marks device d; any thread).
+template <typename Kernel>
+inline void smem_opt_in(Kernel* kernel, size_t bytes, std::atomic<uint64_t>& done) {
+  if (bytes <= 48 * 1024) return;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;  // the launch reports the error
+  const uint64_t bit = dev < 64 ? (uint64_t(1) << dev) : 0;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess && bit)
+    done.fetch_or(bit, std::memory_order_acq_rel);
+}
 
 }  // namespace b200jk

@@ -6,6 +6,7 @@
 #include <unordered_map>
 #include <set>
 #include <functional>
+#include <limits>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -436,6 +437,34 @@ __global__ void split_kernel(const int4* __restrict__ work, const double* __rest
   split[i] = lo;
 }
 
+// Per bra-group work item: max |D| over the rows its quartets touch -- the
+// common A shell, every bra's B shell, every ket's C shell (one warp per item).
+__global__ void grp_split_kernel(const int4* __restrict__ work, int nwork, const int* __restrict__ bord,
+                                 const int4* __restrict__ bix, const int4* __restrict__ bgx,
+                                 const int4* __restrict__ bgy, int gb, const double4* __restrict__ bra,
+                                 const double* __restrict__ kmax, const double* __restrict__ rowmax,
+                                 const int* __restrict__ mol_ao_off, int na, int nb, double* __restrict__ m_out) {
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= nwork) return;
+  const int4 w = work[i];
+  const int p0 = bord[w.x];
+  const int base = mol_ao_off[(int)bra[p0].w];
+  double dmax = 0.0;
+  for (int b = lane; b < w.y; b += 32) {
+    const int pos = bord[w.x + b];
+    const int4 ix = bix[pos];
+    const int4 gx = gb > 1 ? bgx[pos] : make_int4(0, 0, 0, 0);
+    const int4 gy = gb > 1 ? bgy[pos] : make_int4(0, 0, 0, 0);
+    const int ao[4] = {ix.z, gx.z, gy.x, gy.z}, bo[4] = {ix.w, gx.w, gy.y, gy.w};
+    for (int c = 0; c < gb; ++c)
+      dmax = fmax(dmax, fmax(rows_max(rowmax, base, ao[c], na), rows_max(rowmax, base, bo[c], nb)));
+  }
+  for (int k = w.z + lane; k < w.w; k += 32) dmax = fmax(dmax, kmax[k]);
+  for (int off = 16; off > 0; off >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, off));
+  if (lane == 0) m_out[i] = dmax;
+}
+
 // ---------------------------------------------------------------- plan creation
 static int ncart_of(int l) { return (l + 1) * (l + 2) / 2; }
 static int pc_la_host(int pc) { return pc == 0 ? 0 : pc <= 2 ? 1 : pc <= 5 ? 2 : 3; }
@@ -451,6 +480,8 @@ static void validate_tables(const b200jk_molecule& m, int cart) {
     invalid("Invalid libcint table dimensions or operator");
   for (int i = 0; i < m.nenv; ++i)
     if (!std::isfinite(m.env[i])) invalid("Native integral env must be finite");
+  if (m.env[8] > std::sqrt(std::numeric_limits<double>::max()) / 2.0)
+    invalid("omega exceeds the safe float64 squared range");
   // env[8] (libcint PTR_RANGE_OMEGA): omega > 0 selects erf(omega r)/r, as the
   // reference's long-range J/K sets it (plan.py:86-87); the short-range
   // (omega < 0) operator is not built
@@ -504,18 +535,27 @@ struct JKUnit {
   const ClassList* Y;
   int gb, gk;
   std::vector<int4>* h_items;
+  GroupWork* grp;   // non-null: the unit runs the register path over bra groups
 };
 
 template <typename F>
 static void for_each_unit(Plan& p, ClassPairWork& W, F&& f) {
+  auto active = [](GroupWork& G) { return G.h_items.empty() ? &G.all_items : &G.h_items; };
   if (!W.buckets.empty()) {
     const ClassList* X = W.grouped_x ? &p.grouped[W.x] : &p.classes[W.x];
     const ClassList* Y = W.grouped_y ? &p.grouped[W.y] : &p.classes[W.y];
-    for (auto* B : W.buckets)
-      f(JKUnit{&B->work, B->nwork, &B->split, X, Y, B->gb, B->gk, B->h_items.empty() ? &B->all_items : &B->h_items});
+    for (auto* B : W.buckets) {
+      if (B->use_grp)
+        f(JKUnit{&B->grp.work, B->grp.nwork, &B->grp.m, X, Y, B->gb, B->gk, active(B->grp), &B->grp});
+      else
+        f(JKUnit{&B->work, B->nwork, &B->split, X, Y, B->gb, B->gk, B->h_items.empty() ? &B->all_items : &B->h_items,
+                 nullptr});
+    }
+  } else if (W.use_grp) {
+    f(JKUnit{&W.grp.work, W.grp.nwork, &W.grp.m, &p.classes[W.x], &p.classes[W.y], 1, 1, active(W.grp), &W.grp});
   } else {
     f(JKUnit{&W.work, W.nwork, &W.split, &p.classes[W.x], &p.classes[W.y], 1, 1,
-             W.h_items.empty() ? &W.all_items : &W.h_items});
+             W.h_items.empty() ? &W.all_items : &W.h_items, nullptr});
   }
 }
 
@@ -532,6 +572,9 @@ static void set_unit_lists(JKArgs& a, const JKUnit& u, bool same) {
   a.ket_ix = u.Y->d_ix.as<int4>();
   a.ket_gx = u.Y->d_gx.as<int4>();
   a.ket_gy = u.Y->d_gy.as<int4>();
+  a.bra_bord = u.X->d_bord.as<int>();
+  a.bra_q = u.X->d_q.as<double>();
+  a.ket_q = u.Y->d_q.as<double>();
   a.same_list = same;
 }
 
@@ -558,6 +601,7 @@ static JKArgs base_args(const Plan& p) {
   a.mol_n = p.d_mol_ncart.as<int>();
   a.tb = plan_tables(p);
   a.status = p.d_status.as<int>();
+  a.cutoff = p.cutoff;
   return a;
 }
 
@@ -610,6 +654,99 @@ static void upload_items(DevBuf& work, DevBuf& split, const std::vector<int4>& i
   CUDA_OK(split.ensure(std::max<size_t>(items.size(), 1) * sizeof(int)));
 }
 
+#ifndef B200JK_GRP_BRAS
+#define B200JK_GRP_BRAS 16   // bras per bra-group work item
+#endif
+#ifndef B200JK_GRP_CHUNK
+#define B200JK_GRP_CHUNK 64  // kets per bra-group work item
+#endif
+
+// First ket position in [lo, hi) of a Q-descending run with qb * Q < cut.
+static int screen_end(const ClassList& Y, int lo, int hi, double qb, double cut) {
+  if (cut <= 0) return hi;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (qb * Y.q[mid] < cut) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+// Work items of the register path over bra groups: for every group of X's
+// bra order (entries with `gb` combinations) and every ket run of Y in the
+// same molecule (entries with `gk` combinations), the kets any bra of the
+// group meets (its Schwarz prefix, and at most its own position when X and
+// Y are one list), cut into chunks.
+static void fill_group(GroupWork& G, const ClassList& X, const ClassList& Y, bool same, double cut, int chunk,
+                       int gb, int gk) {
+  G.all_items.clear();
+  G.h_items.clear();
+  G.item_cost.clear();
+  G.quartets = G.prim_quartets = 0;
+  auto nco = [](const ClassList& L, int i) { return L.nco.empty() ? 1 : L.nco[i]; };
+  std::vector<int> hp;
+  for (size_t gi = 0; gi + 1 < X.gbeg.size(); ++gi) {
+    const int g0 = X.gbeg[gi], g1 = X.gbeg[gi + 1];
+    const int first = X.bord[g0];
+    if (nco(X, first) != gb) continue;
+    const int m = X.mol_pos[first];
+    for (int c0 = g0; c0 < g1; c0 += B200JK_GRP_BRAS) {
+      const int c1 = std::min(g1, c0 + B200JK_GRP_BRAS);
+      for (const int2 seg : Y.segs[m]) {
+        const int lo = seg.x;
+        if (nco(Y, lo) != gk) continue;
+        hp.assign(c1 - c0, lo);
+        int hi = lo;
+        for (int i = c0; i < c1; ++i) {
+          const int pos = X.bord[i];
+          int h = screen_end(Y, lo, seg.y, X.q[pos], cut);
+          if (same) h = std::min(h, pos + 1);
+          h = std::max(h, lo);
+          hp[i - c0] = h;
+          hi = std::max(hi, h);
+          G.quartets += (long long)(h - lo) * gb * gk;
+          G.prim_quartets += (long long)X.npp_pos[pos] * (Y.npp_prefix[h] - Y.npp_prefix[lo]);
+        }
+        // staircase: the bras a ket meets are the chunk's first cnt(k) bras
+        // (bounds sorted descending); split [lo, hi) where cnt drops, so the
+        // lanes of a pass are mostly active for every bra the item lists --
+        // steps shorter than a pass stay merged with the wider range before
+        // them.  With one list (X == Y) the canonical cap can break the
+        // order; the kernel's per-lane mask covers it.
+        int s = lo;
+        while (s < hi) {
+          int cnt = 0;
+          for (int i = c0; i < c1; ++i)
+            if (hp[i - c0] > s) cnt = i - c0 + 1;
+          if (cnt == 0) break;
+          // the range ends where the first listed bra stops, but runs at least a pass
+          int e = hi;
+          for (int i = c0; i < c0 + cnt; ++i)
+            if (hp[i - c0] > s) e = std::min(e, std::max(hp[i - c0], s + 32));
+          e = std::min(e, hi);
+          for (int b0 = s; b0 < e; b0 += chunk) {
+            const int b1 = std::min(e, b0 + chunk);
+            long long cost = 0;
+            for (int i = c0; i < c0 + cnt; ++i) {
+              const int h = std::min(std::max(hp[i - c0], b0), b1);
+              cost += (long long)X.npp_pos[X.bord[i]] * (Y.npp_prefix[h] - Y.npp_prefix[b0]);
+            }
+            if (cost == 0) continue;
+            G.all_items.push_back(make_int4(c0, cnt, b0, b1));
+            G.item_cost.push_back(cost);
+          }
+          s = e;
+        }
+      }
+    }
+  }
+  G.nwork = (int)G.all_items.size();
+  CUDA_OK(G.work.ensure(std::max<size_t>(G.all_items.size(), 1) * sizeof(int4)));
+  if (!G.all_items.empty())
+    CUDA_OK(cudaMemcpy(G.work.ptr, G.all_items.data(), G.all_items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  CUDA_OK(G.m.ensure(std::max<size_t>(G.all_items.size(), 1) * sizeof(double)));
+}
+
 // (Re)build the work items of class pair W: the expanded items and, where
 // both precisions' kernels take grouped lists, the grouped buckets.
 // `force` > 0 sets the ket chunk of the items the J/K build launches on the
@@ -642,11 +779,16 @@ static void fill_items(Plan& p, ClassPairWork& W, int force) {
     }
   });
   W.nwork = (int)items.size();
+  ++p.layout_gen;
   upload_items(W.work, W.split, items);
   W.h_items.clear();  // unsharded: the active items are all_items
   W.all_items = std::move(items);
   for (auto* B : W.buckets) delete B;
   W.buckets.clear();
+  const bool grp = disp.grp64[cls] && disp.grp32[cls];
+  const int gchunk0 = force > 0 ? force : B200JK_GRP_CHUNK;
+  W.use_grp = grp && !grouped;
+  if (W.use_grp) fill_group(W.grp, X, Y, x == y, cut, gchunk0, 1, 1);
   if (!grouped) return;
   const ClassList& GX = W.grouped_x ? p.grouped[x] : X;
   const ClassList& GY = W.grouped_y ? p.grouped[y] : Y;
@@ -675,6 +817,13 @@ static void fill_items(Plan& p, ClassPairWork& W, int force) {
     B->h_items.clear();
     B->nwork = (int)B->all_items.size();
     upload_items(B->work, B->split, B->all_items);
+    const bool bgrp = (B->gb == 1 && B->gk == 1) ? grp
+                                                    : (disp.grpg64[cls][gen_slot(B->gb, B->gk)] != nullptr &&
+                                                       disp.grpg32[cls][gen_slot(B->gb, B->gk)] != nullptr);
+    if (bgrp) {
+      B->use_grp = true;
+      fill_group(B->grp, GX, GY, x == y, cut, gchunk0, B->gb, B->gk);
+    }
     W.buckets.push_back(B);
   }
 }
@@ -683,6 +832,7 @@ static void fill_items(Plan& p, ClassPairWork& W, int force) {
 // of every item list (expanded items and grouped buckets).
 static void apply_shard(Plan& p, ClassPairWork& W) {
   const int rank = p.shard_rank, world = p.shard_world;
+  ++p.layout_gen;
   auto shard = [&](const std::vector<int4>& all, const std::vector<int64_t>& cost, DevBuf& work,
                    std::vector<int4>& h, int& nwork, long long& q, long long& pq, long long qmul) {
     const int64_t n = (int64_t)all.size();
@@ -707,6 +857,40 @@ static void apply_shard(Plan& p, ClassPairWork& W) {
   for (auto* B : W.buckets)
     shard(B->all_items, B->item_cost, B->work, B->h_items, B->nwork, B->quartets, B->prim_quartets,
           (long long)B->gb * B->gk);
+  // bra-group items: the same contiguous cost-balanced blocks (their quartet
+  // counts stay those of the whole class pair; the expanded items carry the shard's)
+  auto shard_grp = [&](GroupWork& G) {
+    long long q = 0, pq = 0;
+    std::vector<int4> h;
+    int nw = 0;
+    shard(G.all_items, G.item_cost, G.work, h, nw, q, pq, 0);
+    G.h_items = std::move(h);
+    G.nwork = nw;
+  };
+  if (W.use_grp) shard_grp(W.grp);
+  for (auto* B : W.buckets)
+    if (B->use_grp) shard_grp(B->grp);
+}
+
+// Bra order and groups of a class list (register path over bra groups).
+static void build_bra_order(ClassList& L) {
+  const int n = (int)L.q.size();
+  L.bord.resize(n);
+  std::iota(L.bord.begin(), L.bord.end(), 0);
+  auto nco = [&](int i) { return L.nco.empty() ? 1 : L.nco[i]; };
+  auto key_less = [&](int a, int b) {
+    if (L.mol_pos[a] != L.mol_pos[b]) return L.mol_pos[a] < L.mol_pos[b];
+    if (nco(a) != nco(b)) return nco(a) < nco(b);
+    if (L.npp_pos[a] != L.npp_pos[b]) return L.npp_pos[a] < L.npp_pos[b];
+    return L.aoa_pos[a] < L.aoa_pos[b];
+  };
+  // list order breaks ties: Q descending within a group
+  std::sort(L.bord.begin(), L.bord.end(), [&](int a, int b) { return key_less(a, b) || (!key_less(b, a) && a < b); });
+  L.gbeg.clear();
+  for (int i = 0; i < n; ++i)
+    if (i == 0 || key_less(L.bord[i - 1], L.bord[i])) L.gbeg.push_back(i);
+  L.gbeg.push_back(n);
+  upload(L.d_bord, L.bord.data(), (size_t)n * sizeof(int));
 }
 
 // One entry of a grouped list (pair classes (l, 0)): a parent shell pair
@@ -1081,6 +1265,10 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     upload(L.d_ab, ab.data(), ab.size() * sizeof(double4));
     upload(L.d_ix, ix.data(), ix.size() * sizeof(int4));
     CUDA_OK(L.d_kmax.ensure(std::max<size_t>(ids.size(), 1) * sizeof(double)));
+    L.aoa_pos.resize(ids.size());
+    for (size_t i = 0; i < ids.size(); ++i) L.aoa_pos[i] = ix[i].z;
+    build_bra_order(L);
+
   }
   // the combinations of the grouped entries cover exactly the expanded
   // work pairs of their classes (checked once per plan, on the host)
@@ -1173,6 +1361,11 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     upload(L.d_gy, gy.data(), n * sizeof(int4));
     upload(L.d_nco, L.nco.data(), n * sizeof(int));
     CUDA_OK(L.d_kmax.ensure(std::max<size_t>(n, 1) * sizeof(double)));
+    L.aoa_pos.resize(n);
+    for (size_t i = 0; i < n; ++i)
+      L.aoa_pos[i] = (long long)ix[i].z | ((long long)gx[i].z << 16) | ((long long)gy[i].x << 32) |
+                     ((long long)gy[i].z << 48);
+    build_bra_order(L);
   }
   // ---- work items per class pair (X >= Y)
   for (int x = 0; x < kPairClasses; ++x)
@@ -1272,6 +1465,15 @@ static void split_units(Plan& p, ClassPairWork& W, double fp32_cut, cudaStream_t
   for_each_unit(p, W, [&](const JKUnit& u) {
     if (u.nwork == 0) return;  // nothing of this class pair on this shard
     (void)lc;
+    if (u.grp) {
+      grp_split_kernel<<<(u.nwork + 3) / 4, 128, 0, st>>>(
+          u.work->as<int4>(), u.nwork, u.X->d_bord.as<int>(), u.X->d_ix.as<int4>(), u.X->d_gx.as<int4>(),
+          u.X->d_gy.as<int4>(), u.gb, u.X->d_ra.as<double4>(),
+          u.Y->d_kmax.as<double>(), p.d_rowmax.as<double>(), p.d_mol_ao_off.as<int>(), ncart_of(la),
+          ncart_of(lb), u.split->as<double>());
+      CUDA_OK(cudaGetLastError());
+      return;
+    }
     SplitLists L{u.X->d_ix.as<int4>(), u.X->d_gx.as<int4>(), u.X->d_gy.as<int4>(), u.Y->d_kmax.as<double>(),
                  u.X->d_ra.as<double4>(), u.gb, ncart_of(la), ncart_of(lb)};
     split_kernel<<<(u.nwork + 3) / 4, 128, 0, st>>>(u.work->as<int4>(), u.X->d_q.as<double>(),
@@ -1295,10 +1497,14 @@ static void launch_units(Plan& p, ClassPairWork& W, JKArgs a, int precision, cud
     set_unit_lists(a, u, W.x == W.y);
     a.work = u.work->as<int4>();
     a.nwork = u.nwork;
-    a.split = u.split->as<int>();
+    a.split = u.grp ? nullptr : u.split->as<int>();
+    a.item_m = u.grp ? u.split->as<double>() : nullptr;
     const bool plain = u.gb == 1 && u.gk == 1;
-    const JKLauncher l64 = plain ? disp.jk64[cls] : disp.jkg64[cls][gen_slot(u.gb, u.gk)];
-    const JKLauncher l32 = plain ? disp.jk32[cls] : disp.jkg32[cls][gen_slot(u.gb, u.gk)];
+    const int gs = gen_slot(u.gb, u.gk);
+    const JKLauncher l64 = u.grp ? (plain ? disp.grp64[cls] : disp.grpg64[cls][gs])
+                                 : (plain ? disp.jk64[cls] : disp.jkg64[cls][gs]);
+    const JKLauncher l32 = u.grp ? (plain ? disp.grp32[cls] : disp.grpg32[cls][gs])
+                                 : (plain ? disp.jk32[cls] : disp.jkg32[cls][gs]);
     if (!l64 || !l32) throw Failure{B200JK_INTERNAL, "no kernel for this contraction grouping"};
     auto launch = [&](int mode, bool fp32) {
       a.split_mode = mode;
@@ -1366,26 +1572,45 @@ static void launch_all(Plan& p, JKArgs a, int precision, cudaStream_t st) {
 // The J/K pipeline on caller-provided scratch: dens/dens_f hold (hermi ? nb :
 // 2nb) Cartesian matrices, vj nb, vk (hermi ? nb : 2nb); nothing is allocated
 // here when profiling is off.
+// Densities in (output basis) -> raw Cartesian effective densities (status
+// word flags a nonfinite density); J/K accumulators zeroed.
+static void jk_prologue(Plan& p, const double* d_in, int nb, int hermi, int with_j, int with_k,
+                        cudaStream_t st, double* s_dens, double* s_vj, double* s_vk) {
+  const int ndm = hermi ? nb : 2 * nb;
+  const Tables tb = plan_tables(p);
+  const int nc = max_nc(p);
+  const long long n2 = (long long)nc * nc;
+  dim3 grid((unsigned)((n2 + 255) / 256), p.nmol, nb);
+  density_in_kernel<<<grid, 256, 0, st>>>(
+      d_in, nb, hermi, s_dens, p.out_stride, p.cart_stride,
+      p.d_mol_base_out.as<long long>(), p.d_mol_nout.as<int>(), p.d_mol_base_cart.as<long long>(),
+      p.d_mol_ncart.as<int>(), p.d_cart_ws.as<int>(), p.d_ws_info.as<int4>(), p.d_mol_ao_off.as<int>(), tb.c2s,
+      p.d_status.as<int>());
+  CUDA_OK(cudaGetLastError());
+  if (with_j) CUDA_OK(cudaMemsetAsync(s_vj, 0, (size_t)nb * p.cart_stride * sizeof(double), st));
+  if (with_k) CUDA_OK(cudaMemsetAsync(s_vk, 0, (size_t)ndm * p.cart_stride * sizeof(double), st));
+}
+
+// MJ/MK accumulators -> J/K in the output basis (d_out fully overwritten).
+static void jk_epilogue(Plan& p, int nb, int hermi, int with_j, int with_k, double* d_out, cudaStream_t st,
+                        const double* s_vj, const double* s_vk) {
+  const Tables tb = plan_tables(p);
+  const int no = max_no(p);
+  const long long n2 = (long long)no * no;
+  dim3 grid((unsigned)((n2 + 255) / 256), p.nmol, nb);
+  jk_out_kernel<<<grid, 256, 0, st>>>(
+      s_vj, s_vk, nb, hermi, with_j, with_k, d_out, p.out_stride,
+      p.cart_stride, p.d_mol_base_out.as<long long>(), p.d_mol_nout.as<int>(),
+      p.d_mol_base_cart.as<long long>(), p.d_mol_ncart.as<int>(), p.d_out_ws.as<int>(),
+      p.d_ws_info.as<int4>(), p.d_mol_ao_off.as<int>() + p.nmol, tb.c2s);
+  CUDA_OK(cudaGetLastError());
+}
+
 void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j, int with_k,
                  int hermi, int precision, double fp32_cut, cudaStream_t st, double* s_dens,
                  float* s_dens_f, double* s_vj, double* s_vk, bool allow_profiling) {
   const int ndm = hermi ? nb : 2 * nb;
-  const Tables tb = plan_tables(p);
-  const int* d_mol_cart_ao = p.d_mol_ao_off.as<int>();
-  const int* d_mol_out_ao = d_mol_cart_ao + p.nmol;
-  {
-    const int nc = max_nc(p);
-    const long long n2 = (long long)nc * nc;
-    dim3 grid((unsigned)((n2 + 255) / 256), p.nmol, nb);
-    density_in_kernel<<<grid, 256, 0, st>>>(
-        d_in, nb, hermi, s_dens, p.out_stride, p.cart_stride,
-        p.d_mol_base_out.as<long long>(), p.d_mol_nout.as<int>(), p.d_mol_base_cart.as<long long>(),
-        p.d_mol_ncart.as<int>(), p.d_cart_ws.as<int>(), p.d_ws_info.as<int4>(), d_mol_cart_ao, tb.c2s,
-        p.d_status.as<int>());
-    CUDA_OK(cudaGetLastError());
-  }
-  if (with_j) CUDA_OK(cudaMemsetAsync(s_vj, 0, (size_t)nb * p.cart_stride * sizeof(double), st));
-  if (with_k) CUDA_OK(cudaMemsetAsync(s_vk, 0, (size_t)ndm * p.cart_stride * sizeof(double), st));
+  jk_prologue(p, d_in, nb, hermi, with_j, with_k, st, s_dens, s_vj, s_vk);
   if (precision == B200JK_SPLIT) {
     to_float_kernel<<<592, 256, 0, st>>>(s_dens, s_dens_f,
                                          (long long)ndm * p.cart_stride);
@@ -1410,6 +1635,7 @@ void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j,
         CUDA_OK(cudaGetLastError());
       }
     for (auto* W : p.work) split_units(p, *W, fp32_cut, st);
+    p.last_fp32_cut = fp32_cut;
   }
   JKArgs a = base_args(p);
   a.dens = s_dens;
@@ -1421,23 +1647,14 @@ void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j,
   a.nsym = nb;
   a.with_j = with_j;
   a.with_k = with_k;
+  a.fp32_cut = fp32_cut;
   if (p.profiling && allow_profiling) {
     // serial, so that every class-pair launch is timed alone
     for (auto* W : p.work) launch_units(p, *W, a, precision, st, true);
   } else {
     launch_all(p, a, precision, st);
   }
-  {
-    const int no = max_no(p);
-    const long long n2 = (long long)no * no;
-    dim3 grid((unsigned)((n2 + 255) / 256), p.nmol, nb);
-    jk_out_kernel<<<grid, 256, 0, st>>>(
-        s_vj, s_vk, nb, hermi, with_j, with_k, d_out, p.out_stride,
-        p.cart_stride, p.d_mol_base_out.as<long long>(), p.d_mol_nout.as<int>(),
-        p.d_mol_base_cart.as<long long>(), p.d_mol_ncart.as<int>(), p.d_out_ws.as<int>(),
-        p.d_ws_info.as<int4>(), d_mol_out_ao, tb.c2s);
-    CUDA_OK(cudaGetLastError());
-  }
+  jk_epilogue(p, nb, hermi, with_j, with_k, d_out, st, s_vj, s_vk);
 }
 
 static void run_jk(Plan& p, const double* d_in, int nb, double* d_out, int with_j, int with_k,
@@ -1526,10 +1743,17 @@ int b200jk_direct_jk(b200jk_plan* plan, const double* d_density, int32_t nb, dou
   });
 }
 
+// A captured build owns its scratch (effective densities, J/K accumulators),
+// so later calls on the plan with more densities, which grow the plan's own
+// scratch, leave the graph's pointers valid.  The plan's work-item arrays are
+// shared: the graph records their generation and refuses to replay once
+// autotune or set_shard has rebuilt them.
 struct b200jk_graph {
-  b200jk_plan* plan;
-  cudaGraph_t graph;
-  cudaGraphExec_t exec;
+  b200jk_plan* plan = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long layout_gen = 0;
+  DevBuf dens, dens_f, vj, vk;
 };
 
 int b200jk_graph_create(b200jk_plan* plan, const double* d_density, int32_t nb, double* d_out,
@@ -1541,41 +1765,58 @@ int b200jk_graph_create(b200jk_plan* plan, const double* d_density, int32_t nb, 
     Plan& p = *plan->p;
     check_jk_args(p, d_density, nb, d_out, with_j, with_k, precision, fp32_cut);
     CUDA_OK(cudaSetDevice(p.device));
-    ensure_scratch(p, nb);
+    std::unique_ptr<b200jk_graph> g(new b200jk_graph());
+    g->plan = plan;
+    const size_t cs = (size_t)p.cart_stride, ndm = hermi ? (size_t)nb : 2 * (size_t)nb;
+    CUDA_OK(g->dens.ensure(ndm * cs * sizeof(double)));
+    CUDA_OK(g->dens_f.ensure(ndm * cs * sizeof(float)));
+    CUDA_OK(g->vj.ensure((size_t)nb * cs * sizeof(double)));
+    CUDA_OK(g->vk.ensure(ndm * cs * sizeof(double)));
     cudaStream_t st;
     CUDA_OK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    // one eager build first: first-use kernel attributes are set outside capture
-    run_jk_core(p, d_density, nb, d_out, with_j, with_k, hermi ? 1 : 0, precision, fp32_cut, st,
-                p.d_dens.as<double>(), p.d_dens_f.as<float>(), p.d_vj.as<double>(), p.d_vk.as<double>(),
-                false);
-    CUDA_OK(cudaStreamSynchronize(st));
-    cudaGraph_t graph = nullptr;
-    CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    try {
+    auto build = [&] {
       run_jk_core(p, d_density, nb, d_out, with_j, with_k, hermi ? 1 : 0, precision, fp32_cut, st,
-                  p.d_dens.as<double>(), p.d_dens_f.as<float>(), p.d_vj.as<double>(),
-                  p.d_vk.as<double>(), false);
+                  g->dens.as<double>(), g->dens_f.as<float>(), g->vj.as<double>(), g->vk.as<double>(),
+                  false);
+    };
+    // one eager build first: first-use kernel attributes are set outside capture
+    try {
+      build();
     } catch (...) {
-      cudaStreamEndCapture(st, &graph);
-      if (graph) cudaGraphDestroy(graph);
+      cudaStreamSynchronize(st);
       cudaStreamDestroy(st);
       throw;
     }
-    CUDA_OK(cudaStreamEndCapture(st, &graph));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      build();
+    } catch (...) {
+      cudaStreamEndCapture(st, &g->graph);
+      if (g->graph) cudaGraphDestroy(g->graph);
+      g->graph = nullptr;
+      cudaStreamDestroy(st);
+      throw;
+    }
+    CUDA_OK(cudaStreamEndCapture(st, &g->graph));
     cudaStreamDestroy(st);
-    cudaGraphExec_t exec = nullptr;
-    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    const cudaError_t e = cudaGraphInstantiate(&g->exec, g->graph, 0);
     if (e != cudaSuccess) {
-      cudaGraphDestroy(graph);
+      cudaGraphDestroy(g->graph);
+      g->graph = nullptr;
       throw Failure{B200JK_INTERNAL, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
     }
-    *out = new b200jk_graph{plan, graph, exec};
+    g->layout_gen = p.layout_gen;
+    *out = g.release();
   });
 }
 
 int b200jk_graph_launch(b200jk_graph* g, void* stream) {
   return guarded([&] {
     if (!g) invalid("Null graph");
+    if (g->layout_gen != g->plan->p->layout_gen)
+      invalid("The plan's work items were rebuilt (autotune or set_shard) after this graph was "
+              "captured; destroy the graph and create a new one");
     CUDA_OK(cudaSetDevice(g->plan->p->device));
     CUDA_OK(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
   });
@@ -1584,8 +1825,8 @@ int b200jk_graph_launch(b200jk_graph* g, void* stream) {
 void b200jk_graph_destroy(b200jk_graph* g) {
   if (!g) return;
   cudaSetDevice(g->plan->p->device);
-  cudaGraphExecDestroy(g->exec);
-  cudaGraphDestroy(g->graph);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
   delete g;
 }
 
@@ -1608,12 +1849,17 @@ int b200jk_direct_jk_tables(const int32_t* atm, int32_t natm, const int32_t* bas
                             int32_t n, double* d_out, int32_t cart, double cutoff, int32_t workers,
                             int32_t with_j, int32_t with_k, void* stream) {
   return guarded([&] {
+    // the handler's order of checks (csrc/direct_jk.cc:15-24): workers,
+    // operator flags, tables, shapes, then the density values
     if (workers < 1) invalid("Direct J/K workers must be positive");
+    if ((with_j != 0 && with_j != 1) || (with_k != 0 && with_k != 1) || !(with_j || with_k))
+      invalid("Direct J/K requires at least one selected operator");
     int dev = 0;
     CUDA_OK(cudaGetDevice(&dev));
     b200jk_molecule m{atm, natm, bas, nbas, env, nenv};
     std::unique_ptr<Plan> p(build_plan(&m, 1, cart, cutoff, dev));
-    if (n != p->mol_nout[0]) invalid("Direct J/K shape mismatch");
+    if (nb < 0 || n != p->mol_nout[0]) invalid("Direct J/K shape mismatch");
+    if (nb == 0) return;  // an empty batch: the handler writes nothing either
     run_jk(*p, d_density, nb, d_out, with_j, with_k, 0, B200JK_FP64, 0.0, (cudaStream_t)stream);
     CUDA_OK(cudaStreamSynchronize((cudaStream_t)stream));
     int st = 0;
@@ -1669,6 +1915,7 @@ int b200jk_plan_autotune(b200jk_plan* plan, const double* d_density, int32_t nb,
     a.nsym = nb;
     a.with_j = 1;
     a.with_k = 1;
+    a.fp32_cut = fp32_cut;
     const auto& disp = dispatch();
     cudaEvent_t e0, e1;
     CUDA_OK(cudaEventCreate(&e0));
@@ -1711,13 +1958,8 @@ int b200jk_plan_launches(const b200jk_plan* plan, int32_t precision, int64_t* co
     if (!plan || !count) invalid("Invalid plan query");
     const Plan& p = *plan->p;
     long long units = 0, lists = 0;
-    for (auto* W : p.work) {
-      if (!W->buckets.empty()) {
-        for (auto* B : W->buckets) units += B->nwork > 0;
-      } else {
-        units += W->nwork > 0;
-      }
-    }
+    for (auto* W : p.work)
+      for_each_unit(const_cast<Plan&>(p), *W, [&](const JKUnit& u) { units += u.nwork > 0; });
     for (int c = 0; c < kPairClasses; ++c) lists += !p.classes[c].q.empty() + !p.grouped[c].q.empty();
     // density_in + jk_out; split: to_float, maxabs, rowmax, one row-max pass
     // per list, one boundary kernel and two J/K slices per unit
@@ -1769,6 +2011,39 @@ int b200jk_plan_split_stats(b200jk_plan* plan, void* stream, int64_t* q64, int64
       const int c = quartet_class(W->x, W->y);
       for_each_unit(p, *W, [&](const JKUnit& u) {
         if (u.nwork == 0) return;
+        if (u.grp) {
+          // per bra of each item: screened, canonical kets, FP64 while
+          // Q_bra Q_ket M_item >= fp32_cut (a prefix of the Q-descending run)
+          std::vector<double> m(u.nwork);
+          CUDA_OK(cudaMemcpy(m.data(), u.split->ptr, u.nwork * sizeof(double), cudaMemcpyDeviceToHost));
+          const ClassList& X = *u.X;
+          const ClassList& Y = *u.Y;
+          const auto& pre = Y.npp_prefix;
+          const bool same = W->x == W->y;
+          for (int i = 0; i < u.nwork; ++i) {
+            const int4 it = (*u.h_items)[i];
+            for (int b = 0; b < it.y; ++b) {
+              const int pos = X.bord[it.x + b];
+              const double qb = X.q[pos];
+              int h = screen_end(Y, it.z, it.w, qb, p.cutoff);
+              if (same) h = std::min(h, pos + 1);
+              h = std::max(h, it.z);
+              int s = it.z, e = h;  // first FP32 ket
+              while (s < e) {
+                const int mid = (s + e) >> 1;
+                if (qb * Y.q[mid] * m[i] < p.last_fp32_cut) e = mid;
+                else s = mid + 1;
+              }
+              const long long npa = X.npp_pos[pos];
+              const long long combos = (long long)u.gb * u.gk;
+              q64[c] += (s - it.z) * combos;
+              q32[c] += (h - s) * combos;
+              pq64[c] += npa * (pre[s] - pre[it.z]);
+              pq32[c] += npa * (pre[h] - pre[s]);
+            }
+          }
+          return;
+        }
         std::vector<int> split(u.nwork);
         CUDA_OK(cudaMemcpy(split.data(), u.split->ptr, u.nwork * sizeof(int), cudaMemcpyDeviceToHost));
         const auto& pre = u.Y->npp_prefix;
@@ -1956,6 +2231,90 @@ int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_
         CUDA_OK(cudaEventRecord(p.join_ev[i], p.aux[i]));
         CUDA_OK(cudaStreamWaitEvent(st, p.join_ev[i], 0));
       }
+  });
+}
+
+// The geometry-product kernel (mode 0/1: JVP of order 1/2, 2: order-2 VJP)
+// of every class pair's expanded work items, on `a` as prepared by the caller.
+static void launch_geom_all(Plan& p, JKArgs a, int mode, cudaStream_t st) {
+  for (auto* W : p.work) {
+    if (W->nwork == 0) continue;
+    const int la = pc_la_host(W->x), lb = W->x - la * (la + 1) / 2;
+    const int lc = pc_la_host(W->y), ld = W->y - lc * (lc + 1) / 2;
+    if (!geom_smem_bytes(la, lb, lc, ld)) throw Failure{B200JK_UNSUPPORTED, "class too large for the geometry products"};
+    set_lists(a, p, *W);
+    a.work = W->work.as<int4>();
+    a.nwork = W->nwork;
+    a.split_mode = 0;
+    const int rc = launch_geom(a, la, lb, lc, ld, mode, st);
+    if (rc) throw Failure{B200JK_INTERNAL, std::string("geometry product launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+  }
+}
+
+int b200jk_direct_jk_geom_jvp(b200jk_plan* plan, const double* d_density, int32_t nb, int32_t hermi,
+                              const double* d_u, const double* d_v, int32_t with_j, int32_t with_k,
+                              double* d_out, void* stream) {
+  return guarded([&] {
+    if (!plan || !d_density || !d_u || !d_out || nb < 1) invalid("Invalid direct J/K geometry product");
+    if ((with_j != 0 && with_j != 1) || (with_k != 0 && with_k != 1) || !(with_j || with_k))
+      invalid("Invalid direct J/K geometry product");
+    Plan& p = *plan->p;
+    CUDA_OK(cudaSetDevice(p.device));
+    cudaStream_t st = (cudaStream_t)stream;
+    ensure_scratch(p, nb);
+    const int hm = hermi ? 1 : 0;
+    jk_prologue(p, d_density, nb, hm, with_j, with_k, st, p.d_dens.as<double>(), p.d_vj.as<double>(),
+                p.d_vk.as<double>());
+    JKArgs a = base_args(p);
+    a.dens = p.d_dens.as<double>();
+    a.vj = p.d_vj.as<double>();
+    a.vk = p.d_vk.as<double>();
+    a.dstride = p.cart_stride;
+    a.ndm = hm ? nb : 2 * nb;
+    a.nsym = nb;
+    a.with_j = with_j;
+    a.with_k = with_k;
+    a.geo_u = d_u;
+    a.geo_v = d_v;
+    launch_geom_all(p, a, d_v ? 1 : 0, st);
+    jk_epilogue(p, nb, hm, with_j, with_k, d_out, st, p.d_vj.as<double>(), p.d_vk.as<double>());
+  });
+}
+
+int b200jk_direct_jk_geom_hvp(b200jk_plan* plan, const double* d_density, int32_t nb, const double* d_u,
+                              const double* d_cot, int32_t with_j, int32_t with_k, double* d_grad,
+                              void* stream) {
+  return guarded([&] {
+    if (!plan || !d_density || !d_u || !d_cot || !d_grad || nb < 1) invalid("Invalid direct J/K geometry product");
+    if ((with_j != 0 && with_j != 1) || (with_k != 0 && with_k != 1) || !(with_j || with_k))
+      invalid("Invalid direct J/K geometry product");
+    Plan& p = *plan->p;
+    CUDA_OK(cudaSetDevice(p.device));
+    cudaStream_t st = (cudaStream_t)stream;
+    ensure_scratch(p, nb);
+    const Tables tb = plan_tables(p);
+    const int nc = max_nc(p);
+    dim3 grid((unsigned)(((long long)nc * nc + 255) / 256), p.nmol, nb);
+    auto to_raw = [&](const double* src, double* dst) {
+      mat_in_kernel<<<grid, 256, 0, st>>>(src, dst, p.out_stride, p.cart_stride,
+          p.d_mol_base_out.as<long long>(), p.d_mol_nout.as<int>(), p.d_mol_base_cart.as<long long>(),
+          p.d_mol_ncart.as<int>(), p.d_cart_ws.as<int>(), p.d_ws_info.as<int4>(), p.d_mol_ao_off.as<int>(),
+          tb.c2s);
+      CUDA_OK(cudaGetLastError());
+    };
+    to_raw(d_density, p.d_dens.as<double>());
+    if (with_j) to_raw(d_cot, p.d_vj.as<double>());
+    if (with_k) to_raw(d_cot + (size_t)(with_j ? nb : 0) * p.out_stride, p.d_vk.as<double>());
+    CUDA_OK(cudaMemsetAsync(d_grad, 0, (size_t)p.total_atm * 3 * sizeof(double), st));
+    JKArgs a = base_args(p);
+    a.dens = p.d_dens.as<double>();
+    a.dstride = p.cart_stride;
+    a.cot_j = with_j ? p.d_vj.as<double>() : nullptr;
+    a.cot_k = with_k ? p.d_vk.as<double>() : nullptr;
+    a.gnb = nb;
+    a.grad = d_grad;
+    a.geo_u = d_u;
+    launch_geom_all(p, a, 2, st);
   });
 }
 

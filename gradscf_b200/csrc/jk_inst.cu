@@ -51,14 +51,8 @@ int launch_class(const JKArgs& args, cudaStream_t stream) {
   } else if constexpr (P::TILE) {
     using TC = TileCfg<LA, LB, LC, LD, R>;
     constexpr size_t smem = TC::bytes();
-    if (smem > 48 * 1024) {
-      static bool configured = false;
-      if (!configured) {
-        cudaFuncSetAttribute(jk_tile_kernel<LA, LB, LC, LD, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        configured = true;
-      }
-    }
+    static std::atomic<uint64_t> smem_done{0};
+    smem_opt_in(jk_tile_kernel<LA, LB, LC, LD, R>, smem, smem_done);
     jk_tile_kernel<LA, LB, LC, LD, R><<<args.nwork, TC::THREADS, smem, stream>>>(args);
   } else {
     constexpr int TEAM = P::TEAM;
@@ -67,14 +61,8 @@ int launch_class(const JKArgs& args, cudaStream_t stream) {
     int teams = 128 / TEAM;
     while (teams > 1 && per_team * teams > 200 * 1024) --teams;
     const size_t smem = per_team * teams;
-    if (smem > 48 * 1024) {
-      static bool configured = false;
-      if (!configured) {
-        cudaFuncSetAttribute(jk_team_kernel<LA, LB, LC, LD, R, TEAM>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = true;
-      }
-    }
+    static std::atomic<uint64_t> smem_done{0};
+    smem_opt_in(jk_team_kernel<LA, LB, LC, LD, R, TEAM>, smem, smem_done);
     jk_team_kernel<LA, LB, LC, LD, R, TEAM><<<args.nwork, teams * TEAM, smem, stream>>>(args);
   }
   return (int)cudaGetLastError();
@@ -90,15 +78,24 @@ int launch_store(const JKArgs& args, int cart, int layout, double* out, long lon
   int teams = 128 / TEAM;
   while (teams > 1 && per_team * teams > 200 * 1024) --teams;
   const size_t smem = per_team * teams;
-  if (smem > 48 * 1024) {
-    static bool configured = false;
-    if (!configured) {
-      cudaFuncSetAttribute(eri_store_kernel<LA, LB, LC, LD, TEAM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-      configured = true;
-    }
-  }
+  static std::atomic<uint64_t> smem_done{0};
+  smem_opt_in(eri_store_kernel<LA, LB, LC, LD, TEAM>, smem, smem_done);
   eri_store_kernel<LA, LB, LC, LD, TEAM><<<args.nwork, teams * TEAM, smem, stream>>>(args, cart, layout, out, npair);
+  return (int)cudaGetLastError();
+}
+
+template <int LA, int LB, int LC, int LD, typename R>
+int launch_grp(const JKArgs& args, cudaStream_t stream) {
+  if (args.nwork <= 0) return 0;
+  jk_grp_kernel<LA, LB, LC, LD, R><<<(args.nwork + kRegWarps - 1) / kRegWarps, 32 * kRegWarps, 0, stream>>>(args);
+  return (int)cudaGetLastError();
+}
+
+template <int LA, int LB, int LC, int LD, typename R, int GB, int GK>
+int launch_grp_gen(const JKArgs& args, cudaStream_t stream) {
+  if (args.nwork <= 0) return 0;
+  jk_grp_gen_kernel<LA, LB, LC, LD, R, GB, GK>
+      <<<(args.nwork + kRegWarps - 1) / kRegWarps, 32 * kRegWarps, 0, stream>>>(args);
   return (int)cudaGetLastError();
 }
 
@@ -120,14 +117,8 @@ int launch_schwarz(const JKArgs& args, int npairs, int cart, cudaStream_t stream
   int teams = 128 / TEAM;
   while (teams > 1 && per_team * teams > 200 * 1024) --teams;
   const size_t smem = per_team * teams;
-  if (smem > 48 * 1024) {
-    static bool configured = false;
-    if (!configured) {
-      cudaFuncSetAttribute(schwarz_kernel<LA, LB, TEAM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-      configured = true;
-    }
-  }
+  static std::atomic<uint64_t> smem_done{0};
+  smem_opt_in(schwarz_kernel<LA, LB, TEAM>, smem, smem_done);
   const int blocks = (npairs + teams - 1) / teams;
   schwarz_kernel<LA, LB, TEAM><<<blocks, teams * TEAM, smem, stream>>>(args, npairs, cart);
   return (int)cudaGetLastError();
@@ -148,14 +139,8 @@ int launch_grad(const JKArgs& args, cudaStream_t stream) {
   int teams = 128 / TEAM;
   while (teams > 1 && per_team * teams > 200 * 1024) --teams;
   const size_t smem = per_team * teams;
-  if (smem > 48 * 1024) {
-    static bool configured = false;
-    if (!configured) {
-      cudaFuncSetAttribute(grad_team_kernel<LA, LB, LC, LD, TEAM>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      configured = true;
-    }
-  }
+  static std::atomic<uint64_t> smem_done{0};
+  smem_opt_in(grad_team_kernel<LA, LB, LC, LD, TEAM>, smem, smem_done);
   grad_team_kernel<LA, LB, LC, LD, TEAM><<<args.nwork, teams * TEAM, smem, stream>>>(args);
   return (int)cudaGetLastError();
 }
@@ -172,6 +157,19 @@ constexpr bool GROUPED = Policy<XA, XB, YA, YB, float>::REG && Policy<XA, XB, YA
 
 constexpr int gslot(int g) { return g == 1 ? 0 : (g == 2 ? 1 : 2); }
 
+// The register path over bra groups: both precisions on the register path.
+#ifndef B200JK_GRP
+#define B200JK_GRP 1
+#endif
+// The per-lane pass sums (GrpAcc::N values of 32 lanes, 4 warps) stay within
+// 32 KB of static shared memory in FP64.
+constexpr bool GRP = B200JK_GRP && Policy<XA, XB, YA, YB, float>::REG && Policy<XA, XB, YA, YB>::REG &&
+                     GrpAcc<XA, XB, YA, YB>::N <= 32;
+#ifndef B200JK_GRP_GEN
+#define B200JK_GRP_GEN 1
+#endif
+constexpr bool GRP_GEN = B200JK_GRP_GEN && GRP;
+
 template <int GB, int GK>
 void register_gen(DispatchTable& t, int id) {
   constexpr bool okb = GB == 1 || (XB == 0 && (GB == 2 || X == 0));
@@ -179,6 +177,12 @@ void register_gen(DispatchTable& t, int id) {
   if constexpr (GROUPED && okb && okk && !(GB == 1 && GK == 1)) {
     t.jkg64[id][3 * gslot(GB) + gslot(GK)] = &launch_gen<XA, XB, YA, YB, double, GB, GK>;
     t.jkg32[id][3 * gslot(GB) + gslot(GK)] = &launch_gen<XA, XB, YA, YB, float, GB, GK>;
+    // pass sums (N x 32 lanes x 4 warps) beside the FP64 primitive and
+    // coefficient caches (20 KB) within 48 KB of static shared memory
+    if constexpr (GRP_GEN && GrpGenAcc<XA, XB, YA, YB, GB, GK>::N <= 26) {
+      t.grpg64[id][3 * gslot(GB) + gslot(GK)] = &launch_grp_gen<XA, XB, YA, YB, double, GB, GK>;
+      t.grpg32[id][3 * gslot(GB) + gslot(GK)] = &launch_grp_gen<XA, XB, YA, YB, float, GB, GK>;
+    }
   }
 }
 
@@ -190,6 +194,10 @@ void REG_NAME(BRA_CLASS, KET_CLASS)(DispatchTable& t) {
   const int id = X * (X + 1) / 2 + Y;
   t.jk64[id] = &launch_class<XA, XB, YA, YB, double>;
   t.jk32[id] = &launch_class<XA, XB, YA, YB, float>;
+  if constexpr (GRP) {
+    t.grp64[id] = &launch_grp<XA, XB, YA, YB, double>;
+    t.grp32[id] = &launch_grp<XA, XB, YA, YB, float>;
+  }
   t.grad64[id] = &launch_grad<XA, XB, YA, YB>;
   t.store[id] = &launch_store<XA, XB, YA, YB>;
   t.reg_path[id] = Policy<XA, XB, YA, YB, float>::REG || Policy<XA, XB, YA, YB>::REG;

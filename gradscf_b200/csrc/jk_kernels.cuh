@@ -60,8 +60,18 @@ struct JKArgs {
   const double* cot_j;       // raw Cartesian J cotangents [gnb][dstride] (or null)
   const double* cot_k;       // raw Cartesian K cotangents (or null)
   int gnb;                   // density / cotangent batches
+  // bra-group register path: bra order -> list position, Schwarz bounds per
+  // list position, per-item density bound, Schwarz and FP32 cuts
+  const int* bra_bord;
+  const double* bra_q;
+  const double* ket_q;
+  const double* item_m;
+  double cutoff, fp32_cut;
   const int* ws_atm;         // atm row of each work shell's centre
   double* grad;              // (atm rows, 3)
+  // coordinate JVP / Hessian-vector products: directions, (atm rows, 3)
+  const double* geo_u;
+  const double* geo_v;
 };
 
 template <typename R> struct DensSel;
@@ -620,6 +630,312 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
 }
 
 // ---------------------------------------------------------------------------
+// Register path over bra groups.  A work item is (bras [g0, g0 + gn) of the
+// bra order, which share molecule, primitive-pair count and shell A; kets
+// [kb, ke) of one ket run).  Lane = ket; for each 32-ket pass the warp walks
+// the group's bras, so the contributions whose targets are the same for
+// every bra of the pass -- K[a][c], K[a][d] (rows of the common shell A,
+// columns of the lane's ket) and J[c][d] (the lane's ket) -- are summed in
+// registers over the bras (R precision: FP32 quartets accumulate in FP32
+// per pass, i.e. per quartet batch) and added to memory once per pass.
+// Only K[b][c], K[b][d] (rows of each bra's own B) go to memory per quartet,
+// and J[a][b] once per bra and pass after a warp reduction.  The density
+// elements of row block A and of the lane's ket (D_cd, D_ad, D_ac) are read
+// once per pass.  Screening (Q_bra Q_ket >= cut), the canonical order (ket
+// position <= bra position when bra and ket come from one list) and the
+// precision slice (FP32 when Q_bra Q_ket M_item < fp32_cut) are per-lane
+// masks; a bra none of whose quartets is active in the pass is skipped.
+// Densities after the first (nb > 1 or a nonsymmetric density) are
+// digested quartet by quartet.
+// ---------------------------------------------------------------------------
+// One quartet's digestion of density e with every target added to memory.
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void digest_one(const JKArgs& args, const QuartetGeom& g, const R* out, int e) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  constexpr int NA = CI::NA, NB = CI::NB, NC = CI::NC, ND = CI::ND;
+  const double s = g.scale;
+  const long long base = args.mol_base[g.mol];
+  const int n = args.mol_n[g.mol];
+  const R* dm = DensSel<R>::get(args) + e * args.dstride + base;
+  auto dv = [&](int r, int c) -> R { return __ldg(dm + (long long)r * n + c); };
+#define V_(a, b, c, d) (out[(((a) * NB + (b)) * NC + (c)) * ND + (d)])
+  if (args.with_j && e < args.nsym) {
+    double* vj = args.vj + e * args.dstride + base;
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        R acc = R(0);
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+          for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * dv(g.aoC + c, g.aoD + d);
+        atomicAdd(vj + (long long)(g.aoA + a) * n + g.aoB + b, 2.0 * s * double(acc));
+      }
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        R acc = R(0);
+#pragma unroll
+        for (int a = 0; a < NA; ++a)
+#pragma unroll
+          for (int b = 0; b < NB; ++b) acc += V_(a, b, c, d) * dv(g.aoA + a, g.aoB + b);
+        atomicAdd(vj + (long long)(g.aoC + c) * n + g.aoD + d, 2.0 * s * double(acc));
+      }
+  }
+  if (args.with_k) {
+    double* vk = args.vk + e * args.dstride + base;
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        R acc = R(0);
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+#pragma unroll
+          for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * dv(g.aoB + b, g.aoD + d);
+        atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoC + c, s * double(acc));
+      }
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        R acc = R(0);
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+#pragma unroll
+          for (int c = 0; c < NC; ++c) acc += V_(a, b, c, d) * dv(g.aoB + b, g.aoC + c);
+        atomicAdd(vk + (long long)(g.aoA + a) * n + g.aoD + d, s * double(acc));
+      }
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        R acc = R(0);
+#pragma unroll
+        for (int a = 0; a < NA; ++a)
+#pragma unroll
+          for (int d = 0; d < ND; ++d) acc += V_(a, b, c, d) * dv(g.aoA + a, g.aoD + d);
+        atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoC + c, s * double(acc));
+      }
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        R acc = R(0);
+#pragma unroll
+        for (int a = 0; a < NA; ++a)
+#pragma unroll
+          for (int c = 0; c < NC; ++c) acc += V_(a, b, c, d) * dv(g.aoA + a, g.aoC + c);
+        atomicAdd(vk + (long long)(g.aoB + b) * n + g.aoD + d, s * double(acc));
+      }
+  }
+#undef V_
+}
+
+template <int LA, int LB, int LC, int LD>
+struct GrpAcc {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  // per-lane sums over a pass: J[c][d], K[a][c], K[a][d]
+  static constexpr int OJ = 0, OKC = CI::NC * CI::ND, OKD = OKC + CI::NA * CI::NC, N = OKD + CI::NA * CI::ND;
+};
+
+template <int LA, int LB, int LC, int LD, typename R>
+__global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
+    jk_grp_kernel(JKArgs args) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using GA = GrpAcc<LA, LB, LC, LD>;
+  using PA_t = typename PrimData<R>::A;
+  using PB_t = typename PrimData<R>::B;
+  constexpr int NA = CI::NA, NB = CI::NB, NC = CI::NC, ND = CI::ND;
+  __shared__ PA_t s_pp[kRegWarps][kBraPrimCache];
+  __shared__ PB_t s_aux[kRegWarps][kBraPrimCache];
+  // the pass sums live in shared memory, one private column per lane
+  __shared__ R s_acc[kRegWarps][GA::N <= 32 ? GA::N : 1][32];
+  constexpr bool kSharedBoys = sizeof(R) == 4 && CI::NROOT <= 3;
+  __shared__ __align__(16) float s_boys[kSharedBoys ? 401 * 8 : 4];
+  if constexpr (kSharedBoys) {
+    const float4* src = reinterpret_cast<const float4*>(args.tb.boys_s_f + (CI::NROOT - 1) * 401 * 8);
+    float4* dst = reinterpret_cast<float4*>(s_boys);
+    for (int i = threadIdx.x; i < 401 * 2; i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.x * kRegWarps + warp;
+  if (item >= args.nwork) return;
+  const int4 w = args.work[item];  // (bra-order begin, bra count, ket begin, ket end)
+  const double qm = args.split_mode != 0 ? args.item_m[item] : 0.0;
+  const double cut = args.cutoff;
+  const int* __restrict__ bord = args.bra_bord;
+  // the common A shell: Cartesian offset and molecule from the first bra
+  const int p0 = bord[w.x];
+  const int aoA = args.bra_ix[p0].z;
+  const int mol = (int)args.bra_ra[p0].w;
+  const long long mbase = args.mol_base[mol];
+  const int n = args.mol_n[mol];
+  const R* dm0 = DensSel<R>::get(args) + mbase;
+  auto dv = [&](int r, int c) -> R { return __ldg(dm0 + (long long)r * n + c); };
+  const bool doj = args.with_j != 0 && args.nsym > 0, dok = args.with_k != 0;
+  R(*acc)[32] = s_acc[warp];
+  for (int k0 = w.z; k0 < w.w; k0 += 32) {
+    const bool valid = k0 + lane < w.w;
+    const int k = valid ? k0 + lane : w.w - 1;
+    const double qk = args.ket_q[k];
+    const double4 kra = args.ket_ra[k], kab = args.ket_ab[k];
+    const int4 kix = args.ket_ix[k];
+    const int aoC = kix.z, aoD = kix.w;
+#pragma unroll
+    for (int i = 0; i < GA::N; ++i) acc[i][lane] = R(0);
+    bool any = false;
+    for (int bi = 0; bi < w.y; ++bi) {
+      const int pos = bord[w.x + bi];
+      const double qq = args.bra_q[pos] * qk;
+      bool act = valid && qq >= cut && (!args.same_list || k <= pos);
+      if (args.split_mode == 1) act = act && !(qq * qm < args.fp32_cut);
+      else if (args.split_mode == 2) act = act && (qq * qm < args.fp32_cut);
+      if (!__any_sync(0xffffffffu, act)) continue;
+      any = any || act;
+      const BraRec br = load_bra(args, pos);
+      const int ppb = br.ix.x, npb = br.ix.y;
+      const bool cached = npb <= kBraPrimCache;
+      __syncwarp();
+      if (cached)
+        for (int i = lane; i < npb; i += 32) {
+          s_pp[warp][i] = PrimData<R>::a(args, ppb + i);
+          s_aux[warp][i] = PrimData<R>::b(args, ppb + i);
+        }
+      __syncwarp();
+      const PA_t* bpp = cached ? s_pp[warp] : (sizeof(R) == 4 ? (const PA_t*)(args.pp_f + ppb)
+                                                             : (const PA_t*)(args.pp_data + ppb));
+      const PB_t* baux = cached ? s_aux[warp] : (sizeof(R) == 4 ? (const PB_t*)(args.pp_f2 + ppb)
+                                                               : (const PB_t*)(args.pp_aux + ppb));
+      QuartetGeom g;
+      g.A = g.B = g.C = g.D = -1;
+      g.ppa = ppb; g.npa = npb; g.ppc = kix.x; g.npc = kix.y;
+      g.ax = br.ra.x; g.ay = br.ra.y; g.az = br.ra.z;
+      g.cx = kra.x; g.cy = kra.y; g.cz = kra.z;
+      g.abx = br.ab.x; g.aby = br.ab.y; g.abz = br.ab.z;
+      g.cdx = kab.x; g.cdy = kab.y; g.cdz = kab.z;
+      g.aoA = aoA; g.aoB = br.ix.w; g.aoC = aoC; g.aoD = aoD;
+      g.mol = mol;
+      g.scale = (aoA == br.ix.w ? 0.5 : 1.0) * (aoC == aoD ? 0.5 : 1.0) * (args.same_list && k == pos ? 0.5 : 1.0);
+      g.omega2 = args.omega2;
+      R out[CI::NOUT];
+      quartet_block_reg<LA, LB, LC, LD, R>(args, g, bpp, baux, out, s_boys);
+      const int aoB = br.ix.w;
+      const R sR = act ? R(g.scale) : R(0);
+#define V_(a, b, c, d) (out[(((a) * NB + (b)) * NC + (c)) * ND + (d)])
+      if (doj) {
+        // J[a][b] of this bra: warp-reduced, one add per element and pass
+        double* vj = args.vj + mbase;
+#pragma unroll
+        for (int a = 0; a < NA; ++a)
+#pragma unroll
+          for (int b = 0; b < NB; ++b) {
+            R s = R(0);
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+#pragma unroll
+              for (int d = 0; d < ND; ++d) s += V_(a, b, c, d) * dv(aoC + c, aoD + d);
+            double v = 2.0 * double(sR) * double(s);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0 && v != 0.0) atomicAdd(vj + (long long)(aoA + a) * n + aoB + b, v);
+          }
+        // J[c][d] of the lane's ket, summed over the bras
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+          for (int d = 0; d < ND; ++d) {
+            R s = R(0);
+#pragma unroll
+            for (int a = 0; a < NA; ++a)
+#pragma unroll
+              for (int b = 0; b < NB; ++b) s += V_(a, b, c, d) * dv(aoA + a, aoB + b);
+            acc[GA::OJ + c * ND + d][lane] += R(2) * sR * s;
+          }
+      }
+      if (dok) {
+        double* vk = args.vk + mbase;
+        // K[a][c] += s sum_bd V D_bd, K[a][d] += s sum_bc V D_bc (pass sums)
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            R s = R(0);
+#pragma unroll
+            for (int b = 0; b < NB; ++b)
+#pragma unroll
+              for (int d = 0; d < ND; ++d) s += V_(a, b, c, d) * dv(aoB + b, aoD + d);
+            acc[GA::OKC + a * NC + c][lane] += sR * s;
+          }
+#pragma unroll
+          for (int d = 0; d < ND; ++d) {
+            R s = R(0);
+#pragma unroll
+            for (int b = 0; b < NB; ++b)
+#pragma unroll
+              for (int c = 0; c < NC; ++c) s += V_(a, b, c, d) * dv(aoB + b, aoC + c);
+            acc[GA::OKD + a * ND + d][lane] += sR * s;
+          }
+        }
+        // K[b][c], K[b][d]: rows of this bra's B, added per quartet
+        if (act) {
+#pragma unroll
+          for (int b = 0; b < NB; ++b) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              R s = R(0);
+#pragma unroll
+              for (int a = 0; a < NA; ++a)
+#pragma unroll
+                for (int d = 0; d < ND; ++d) s += V_(a, b, c, d) * dv(aoA + a, aoD + d);
+              atomicAdd(vk + (long long)(aoB + b) * n + aoC + c, double(sR) * double(s));
+            }
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+              R s = R(0);
+#pragma unroll
+              for (int a = 0; a < NA; ++a)
+#pragma unroll
+                for (int c = 0; c < NC; ++c) s += V_(a, b, c, d) * dv(aoA + a, aoC + c);
+              atomicAdd(vk + (long long)(aoB + b) * n + aoD + d, double(sR) * double(s));
+            }
+          }
+        }
+      }
+#undef V_
+      if (act)
+        for (int e = 1; e < args.ndm; ++e) digest_one<LA, LB, LC, LD, R>(args, g, out, e);
+    }
+    // the pass sums of density 0: J[c][d], K[a][c], K[a][d]
+    if (any) {
+      if (doj) {
+        double* vj = args.vj + mbase;
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+          for (int d = 0; d < ND; ++d)
+            atomicAdd(vj + (long long)(aoC + c) * n + aoD + d, double(acc[GA::OJ + c * ND + d][lane]));
+      }
+      if (dok) {
+        double* vk = args.vk + mbase;
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c)
+            atomicAdd(vk + (long long)(aoA + a) * n + aoC + c, double(acc[GA::OKC + a * NC + c][lane]));
+#pragma unroll
+          for (int d = 0; d < ND; ++d)
+            atomicAdd(vk + (long long)(aoA + a) * n + aoD + d, double(acc[GA::OKD + a * ND + d][lane]));
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Register path on grouped lists: a bra entry carries GB contraction
 // combinations of its parent shell pair and a ket entry GK; the primitive
 // pairs are shared by the combinations and carry their coefficients
@@ -825,6 +1141,270 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
         const double v = s_jab[warp][b * CI::NAB + ab];
         if (v != 0.0) atomicAdd(vj + (long long)(aoA[b] + ab / CI::NB) * n + aoB[b] + ab % CI::NB, v);
       }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The register path over bra groups on grouped lists: bra entries carry GB
+// contraction combinations (whose A shells the whole group shares) and ket
+// entries GK; each primitive quartet is evaluated once for all GB x GK
+// combination blocks (quartet_block_gen), and every block is digested as in
+// jk_grp_kernel: J[c][d], K[a][c], K[a][d] summed per lane over the pass's
+// bras, one sum set per (bra combination, ket combination).
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD, int GB, int GK>
+struct GrpGenAcc {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  static constexpr int OJ = 0;                                  // [GK][NC*ND]
+  static constexpr int OKC = GK * CI::NC * CI::ND;              // [GB][GK][NA*NC]
+  static constexpr int OKD = OKC + GB * GK * CI::NA * CI::NC;   // [GB][GK][NA*ND]
+  static constexpr int N = OKD + GB * GK * CI::NA * CI::ND;
+};
+
+template <int LA, int LB, int LC, int LD, typename R, int GB, int GK>
+__global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
+                                                     (GB * GK + 1) * ClassInfo<LA, LB, LC, LD>::NOUT>::value))
+    jk_grp_gen_kernel(JKArgs args) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using GA = GrpGenAcc<LA, LB, LC, LD, GB, GK>;
+  using PA_t = typename PrimData<R>::A;
+  using PB_t = typename PrimData<R>::B;
+  using C4 = typename CoefSel<R>::T;
+  constexpr int NA = CI::NA, NB = CI::NB, NC = CI::NC, ND = CI::ND, NO = CI::NOUT;
+  __shared__ PA_t s_pp[kRegWarps][kBraPrimCache];
+  __shared__ PB_t s_aux[kRegWarps][kBraPrimCache];
+  __shared__ C4 s_co[kRegWarps][kBraPrimCache];
+  __shared__ R s_acc[kRegWarps][GA::N <= 26 ? GA::N : 1][32];
+  constexpr bool kSharedBoys = sizeof(R) == 4 && CI::NROOT <= 3;
+  __shared__ __align__(16) float s_boys[kSharedBoys ? 401 * 8 : 4];
+  if constexpr (kSharedBoys) {
+    const float4* src = reinterpret_cast<const float4*>(args.tb.boys_s_f + (CI::NROOT - 1) * 401 * 8);
+    float4* dst = reinterpret_cast<float4*>(s_boys);
+    for (int i = threadIdx.x; i < 401 * 2; i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.x * kRegWarps + warp;
+  if (item >= args.nwork) return;
+  const int4 w = args.work[item];  // (bra-order begin, bra count, ket begin, ket end)
+  const double qm = args.split_mode != 0 ? args.item_m[item] : 0.0;
+  const double cut = args.cutoff;
+  const int* __restrict__ bord = args.bra_bord;
+  // the group's A shells, one per bra combination (shared by every bra of the group)
+  const int p0 = bord[w.x];
+  int aoA[GB];
+  {
+    const int4 ix = args.bra_ix[p0];
+    int4 gx = make_int4(0, 0, 0, 0), gy = make_int4(0, 0, 0, 0);
+    if constexpr (GB > 1) {
+      gx = args.bra_gx[p0];
+      gy = args.bra_gy[p0];
+    }
+    const int a4[4] = {ix.z, gx.z, gy.x, gy.z};
+#pragma unroll
+    for (int b = 0; b < GB; ++b) aoA[b] = a4[b];
+  }
+  const int mol = (int)args.bra_ra[p0].w;
+  const long long mbase = args.mol_base[mol];
+  const int n = args.mol_n[mol];
+  const R* dm0 = DensSel<R>::get(args) + mbase;
+  auto dv = [&](int r, int c) -> R { return __ldg(dm0 + (long long)r * n + c); };
+  const bool doj = args.with_j != 0 && args.nsym > 0, dok = args.with_k != 0;
+  R(*acc)[32] = s_acc[warp];
+  for (int k0 = w.z; k0 < w.w; k0 += 32) {
+    const bool valid = k0 + lane < w.w;
+    const int k = valid ? k0 + lane : w.w - 1;
+    const double qk = args.ket_q[k];
+    const double4 kra = args.ket_ra[k], kab = args.ket_ab[k];
+    const int4 kix = args.ket_ix[k];
+    int aoC[GK], aoD[GK];
+    bool kdiag;
+    {
+      int4 gx = make_int4(kix.z == kix.w, 0, 0, 0), gy = make_int4(0, 0, 0, 0);
+      if constexpr (GK > 1) {
+        gx = args.ket_gx[k];
+        gy = args.ket_gy[k];
+      }
+      const int c4[4] = {kix.z, gx.z, gy.x, gy.z}, d4[4] = {kix.w, gx.w, gy.y, gy.w};
+#pragma unroll
+      for (int c = 0; c < GK; ++c) { aoC[c] = c4[c]; aoD[c] = d4[c]; }
+      kdiag = gx.x != 0;
+    }
+#pragma unroll
+    for (int i = 0; i < GA::N; ++i) acc[i][lane] = R(0);
+    bool any = false;
+    for (int bi = 0; bi < w.y; ++bi) {
+      const int pos = bord[w.x + bi];
+      const double qq = args.bra_q[pos] * qk;
+      bool act = valid && qq >= cut && (!args.same_list || k <= pos);
+      if (args.split_mode == 1) act = act && !(qq * qm < args.fp32_cut);
+      else if (args.split_mode == 2) act = act && (qq * qm < args.fp32_cut);
+      if (!__any_sync(0xffffffffu, act)) continue;
+      any = any || act;
+      const BraRec br = load_bra(args, pos);
+      const int ppb = br.ix.x, npb = br.ix.y;
+      int aoB[GB];
+      bool bdiag;
+      {
+        int4 gx = make_int4(br.ix.z == br.ix.w, 0, 0, 0), gy = make_int4(0, 0, 0, 0);
+        if constexpr (GB > 1) {
+          gx = args.bra_gx[pos];
+          gy = args.bra_gy[pos];
+        }
+        const int b4[4] = {br.ix.w, gx.w, gy.y, gy.w};
+#pragma unroll
+        for (int b = 0; b < GB; ++b) aoB[b] = b4[b];
+        bdiag = gx.x != 0;
+      }
+      const bool cached = npb <= kBraPrimCache;
+      __syncwarp();
+      if (cached)
+        for (int i = lane; i < npb; i += 32) {
+          s_pp[warp][i] = PrimData<R>::a(args, ppb + i);
+          s_aux[warp][i] = PrimData<R>::b(args, ppb + i);
+          s_co[warp][i] = CoefSel<R>::get(args, ppb + i);
+        }
+      __syncwarp();
+      const PA_t* bpp = cached ? s_pp[warp] : (sizeof(R) == 4 ? (const PA_t*)(args.pp_f + ppb)
+                                                             : (const PA_t*)(args.pp_data + ppb));
+      const PB_t* baux = cached ? s_aux[warp] : (sizeof(R) == 4 ? (const PB_t*)(args.pp_f2 + ppb)
+                                                               : (const PB_t*)(args.pp_aux + ppb));
+      const C4* bco = cached ? s_co[warp] : (sizeof(R) == 4 ? (const C4*)(args.pp_cf + ppb)
+                                                           : (const C4*)(args.pp_c + ppb));
+      QuartetGeom g;
+      g.A = g.B = g.C = g.D = -1;
+      g.ppa = ppb; g.npa = npb; g.ppc = kix.x; g.npc = kix.y;
+      g.ax = br.ra.x; g.ay = br.ra.y; g.az = br.ra.z;
+      g.cx = kra.x; g.cy = kra.y; g.cz = kra.z;
+      g.abx = br.ab.x; g.aby = br.ab.y; g.abz = br.ab.z;
+      g.cdx = kab.x; g.cdy = kab.y; g.cdz = kab.z;
+      g.mol = mol;
+      g.omega2 = args.omega2;
+      const double sbk = (bdiag ? 0.5 : 1.0) * (kdiag ? 0.5 : 1.0) * (args.same_list && k == pos ? 0.5 : 1.0);
+      R out[GB * GK * NO];
+      quartet_block_gen<LA, LB, LC, LD, R, GB, GK>(args, g, bpp, baux, bco, out, s_boys);
+      const R sR = act ? R(sbk) : R(0);
+#pragma unroll
+      for (int b = 0; b < GB; ++b)
+#pragma unroll
+        for (int c = 0; c < GK; ++c) {
+          const R* o = out + (b * GK + c) * NO;
+          const int oA = aoA[b], oB = aoB[b], oC = aoC[c], oD = aoD[c];
+#define V_(a, bb, cc, d) (o[(((a) * NB + (bb)) * NC + (cc)) * ND + (d)])
+          if (doj) {
+            double* vj = args.vj + mbase;
+#pragma unroll
+            for (int a = 0; a < NA; ++a)
+#pragma unroll
+              for (int bb = 0; bb < NB; ++bb) {
+                R s = R(0);
+#pragma unroll
+                for (int cc = 0; cc < NC; ++cc)
+#pragma unroll
+                  for (int d = 0; d < ND; ++d) s += V_(a, bb, cc, d) * dv(oC + cc, oD + d);
+                double v = 2.0 * double(sR) * double(s);
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+                if (lane == 0 && v != 0.0) atomicAdd(vj + (long long)(oA + a) * n + oB + bb, v);
+              }
+#pragma unroll
+            for (int cc = 0; cc < NC; ++cc)
+#pragma unroll
+              for (int d = 0; d < ND; ++d) {
+                R s = R(0);
+#pragma unroll
+                for (int a = 0; a < NA; ++a)
+#pragma unroll
+                  for (int bb = 0; bb < NB; ++bb) s += V_(a, bb, cc, d) * dv(oA + a, oB + bb);
+                acc[GA::OJ + c * NC * ND + cc * ND + d][lane] += R(2) * sR * s;
+              }
+          }
+          if (dok) {
+            double* vk = args.vk + mbase;
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+#pragma unroll
+              for (int cc = 0; cc < NC; ++cc) {
+                R s = R(0);
+#pragma unroll
+                for (int bb = 0; bb < NB; ++bb)
+#pragma unroll
+                  for (int d = 0; d < ND; ++d) s += V_(a, bb, cc, d) * dv(oB + bb, oD + d);
+                acc[GA::OKC + (b * GK + c) * NA * NC + a * NC + cc][lane] += sR * s;
+              }
+#pragma unroll
+              for (int d = 0; d < ND; ++d) {
+                R s = R(0);
+#pragma unroll
+                for (int bb = 0; bb < NB; ++bb)
+#pragma unroll
+                  for (int cc = 0; cc < NC; ++cc) s += V_(a, bb, cc, d) * dv(oB + bb, oC + cc);
+                acc[GA::OKD + (b * GK + c) * NA * ND + a * ND + d][lane] += sR * s;
+              }
+            }
+            if (act) {
+#pragma unroll
+              for (int bb = 0; bb < NB; ++bb) {
+#pragma unroll
+                for (int cc = 0; cc < NC; ++cc) {
+                  R s = R(0);
+#pragma unroll
+                  for (int a = 0; a < NA; ++a)
+#pragma unroll
+                    for (int d = 0; d < ND; ++d) s += V_(a, bb, cc, d) * dv(oA + a, oD + d);
+                  atomicAdd(vk + (long long)(oB + bb) * n + oC + cc, double(sR) * double(s));
+                }
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                  R s = R(0);
+#pragma unroll
+                  for (int a = 0; a < NA; ++a)
+#pragma unroll
+                    for (int cc = 0; cc < NC; ++cc) s += V_(a, bb, cc, d) * dv(oA + a, oC + cc);
+                  atomicAdd(vk + (long long)(oB + bb) * n + oD + d, double(sR) * double(s));
+                }
+              }
+            }
+          }
+#undef V_
+          if (act) {
+            QuartetGeom gc = g;
+            gc.aoA = oA; gc.aoB = oB; gc.aoC = oC; gc.aoD = oD;
+            gc.scale = sbk;
+            for (int e = 1; e < args.ndm; ++e) digest_one<LA, LB, LC, LD, R>(args, gc, o, e);
+          }
+        }
+    }
+    if (any) {
+      if (doj) {
+        double* vj = args.vj + mbase;
+#pragma unroll
+        for (int c = 0; c < GK; ++c)
+#pragma unroll
+          for (int cc = 0; cc < NC; ++cc)
+#pragma unroll
+            for (int d = 0; d < ND; ++d)
+              atomicAdd(vj + (long long)(aoC[c] + cc) * n + aoD[c] + d, double(acc[GA::OJ + c * NC * ND + cc * ND + d][lane]));
+      }
+      if (dok) {
+        double* vk = args.vk + mbase;
+#pragma unroll
+        for (int b = 0; b < GB; ++b)
+#pragma unroll
+          for (int c = 0; c < GK; ++c)
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+#pragma unroll
+              for (int cc = 0; cc < NC; ++cc)
+                atomicAdd(vk + (long long)(aoA[b] + a) * n + aoC[c] + cc,
+                          double(acc[GA::OKC + (b * GK + c) * NA * NC + a * NC + cc][lane]));
+#pragma unroll
+              for (int d = 0; d < ND; ++d)
+                atomicAdd(vk + (long long)(aoA[b] + a) * n + aoD[c] + d,
+                          double(acc[GA::OKD + (b * GK + c) * NA * ND + a * ND + d][lane]));
+            }
+      }
+    }
   }
 }
 

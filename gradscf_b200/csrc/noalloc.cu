@@ -15,9 +15,14 @@
 // contents (the J/K accumulators are zeroed at the start of every call), so
 // two calls whose work overlaps on the GPU -- different streams, or
 // different threads without ordering -- race and corrupt each other's
-// results; order them on one stream.  The first call on each device looks
-// up the array's device address (cudaGetSymbolAddress) with that device
-// current; make that first call before any stream capture.
+// results; order them on one stream.  A call also uses the plan's own small
+// device state (density row maxima, status word, per-item FP32 boundaries,
+// auxiliary streams), so it races with any other build on the same plan
+// (b200jk_direct_jk, a graph replay, the geometry VJP) that overlaps it on
+// the GPU.  The first call on each device looks up the array's device
+// address (cudaGetSymbolAddress) with that device current; make that first
+// call before any stream capture.  The caller's current device is restored
+// on return.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -77,7 +82,14 @@ extern "C" int b200jk_direct_jk_noalloc(b200jk_plan* plan, const double* d_densi
                    " bytes of scratch, above the fixed " +
                    std::to_string((size_t)B200JK_NOALLOC_SCRATCH_BYTES) +
                    " bytes; use b200jk_direct_jk (which allocates) or fewer densities");
+    int caller_device = 0;
+    if (cudaGetDevice(&caller_device) != cudaSuccess) fail_invalid("cannot read the current device");
     if (cudaSetDevice(p.device) != cudaSuccess) fail_invalid("cannot select the plan's device");
+    // the caller's device is current again when this scope ends, on every path
+    struct RestoreDevice {
+      int dev;
+      ~RestoreDevice() { cudaSetDevice(dev); }
+    } restore{caller_device};
     double* base = scratch_address(p.device);
     double* s_dens = base;
     float* s_dens_f = n_dens_f ? reinterpret_cast<float*>(base + n_dens) : nullptr;

@@ -33,6 +33,19 @@ struct DevBuf {
   template <typename T> T* as() const { return static_cast<T*>(ptr); }
 };
 
+// Work items of the register path over bra groups (jk_grp_kernel): int4
+// (bra-order begin, bra count, ket begin, ket end), the bras sharing
+// molecule, combinations, primitive-pair count and shell A, the kets one run
+// of equal primitive-pair count; `m` holds each item's density bound (max |D|
+// over the rows its quartets touch) for split-precision calls.
+struct GroupWork {
+  int nwork = 0;
+  DevBuf work, m;
+  std::vector<int4> h_items, all_items;
+  std::vector<int64_t> item_cost;
+  long long quartets = 0, prim_quartets = 0;
+};
+
 // Work items of a class pair on grouped lists whose bra / ket entries carry
 // gb / gk contraction combinations (one kernel instantiation per bucket).
 struct GenBucket {
@@ -42,6 +55,8 @@ struct GenBucket {
   std::vector<int4> h_items, all_items;
   std::vector<int64_t> item_cost;
   long long quartets = 0, prim_quartets = 0;
+  bool use_grp = false;   // the bucket runs the bra-group register path
+  GroupWork grp;
 };
 
 struct ClassPairWork {
@@ -60,6 +75,8 @@ struct ClassPairWork {
   bool grouped_x = false, grouped_y = false;
   int chunk = 0;                // register-path ket chunk chosen by the autotuner (0: default rule)
   std::vector<GenBucket*> buckets;
+  bool use_grp = false;         // J/K on the bra-group register path (no buckets)
+  GroupWork grp;
   ~ClassPairWork() {
     for (auto* b : buckets) delete b;
   }
@@ -83,6 +100,13 @@ struct ClassList {
   std::vector<int> nco;
   DevBuf d_gx, d_gy, d_nco;
   DevBuf d_kmax;  // per position: max |D| over the rows of its A shell (split calls)
+  // bra order of the bra-group register path: positions sorted by (molecule,
+  // combinations, primitive pairs, Cartesian offsets of the combinations' A
+  // shells (aoa_pos packs up to four 16-bit offsets), Q desc); gbeg holds the
+  // first bra-order index of every group of equal keys (+ the end)
+  std::vector<long long> aoa_pos;
+  std::vector<int> bord, gbeg;
+  DevBuf d_bord;
 };
 
 struct ProfileEvent {
@@ -145,6 +169,10 @@ struct Plan {
   // scratch
   DevBuf d_dens, d_dens_f, d_vj, d_vk;
   int scratch_nb = 0;
+  // bumped whenever device work-item arrays are rebuilt or rewritten
+  // (autotune, set_shard): a CUDA graph captured before then is stale
+  unsigned long long layout_gen = 0;
+  double last_fp32_cut = 0.0;   // fp32_cut of the last split-precision build (split statistics)
   // optional per-class launch timing (CUDA events on the launching stream)
   bool profiling = false;
   std::vector<ProfileEvent> events;
@@ -168,6 +196,10 @@ void run_jk_core(Plan& p, const double* d_in, int nb, double* d_out, int with_j,
                  int hermi, int precision, double fp32_cut, cudaStream_t st, double* s_dens,
                  float* s_dens_f, double* s_vj, double* s_vk, bool allow_profiling);
 int guarded_call(const std::function<void()>& f);
+// coordinate JVP (mode 0: order 1, 1: order 2) and order-2 VJP (mode 2) of
+// one class pair's expanded work items (geom.cu)
+int launch_geom(const JKArgs& args, int la, int lb, int lc, int ld, int mode, cudaStream_t st);
+size_t geom_smem_bytes(int la, int lb, int lc, int ld);
 void fail_invalid(const std::string& m);
 
 // Device-wide constant tables (Rys, Boys, c2s) of the current device.

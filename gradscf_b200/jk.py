@@ -276,6 +276,93 @@ def direct_jk(atm, bas, env, density, *, cart, cutoff=0.0, workers=1, with_j=Tru
     return (out[0] if with_j else torch.zeros_like(d), out[-1] if with_k else torch.zeros_like(d))
 
 
+def _coordinate_rows(atm, vector, dev):
+    """env-sized coordinate direction -> (natm, 3) rows per atm row.  Only the
+    coordinate slots may be nonzero (csrc/direct_jk_geometry.cc:35-48)."""
+    v = np.asarray(vector, dtype=np.float64)
+    if v.ndim != 1:
+        raise ValueError("Direct J/K geometry direction shape mismatch")
+    if not np.all(np.isfinite(v)):
+        raise ValueError("Direct J/K geometry input must be finite")
+    a = np.asarray(atm)
+    slots = (a[:, 1].astype(np.int64)[:, None] + np.arange(3)[None, :])
+    allowed = np.zeros(v.shape[0], dtype=bool)
+    allowed[slots.ravel()] = True
+    if np.any(v[~allowed] != 0.0):
+        raise ValueError("Direct J/K geometry supports coordinates only, not basis exponents/coefficients")
+    return torch.as_tensor(v[slots], device=dev).contiguous(), slots
+
+
+def _geometry_setup(atm, bas, env, density, cart, cutoff, with_j, with_k, dev):
+    if not (with_j or with_k):
+        raise ValueError("Invalid direct J/K geometry product")
+    dev = torch.device("cuda", torch.cuda.current_device()) if dev is None else torch.device(dev)
+    d = torch.as_tensor(density, dtype=torch.float64, device=dev)
+    n = d.shape[-1]
+    if d.dim() < 2 or d.shape[-2:] != (n, n) or not torch.isfinite(d).all():
+        raise ValueError("Direct J/K geometry input must be finite (..., n, n) float64")
+    plan = cached_plan(atm, bas, env, cart=cart, cutoff=cutoff, device=dev)
+    if plan.nao[0] != n:
+        raise ValueError("Direct J/K geometry density shape mismatch")
+    return plan, d, n, dev
+
+
+def direct_jk_geometry_jvp(atm, bas, env, density, direction, vector=None, *, cart, cutoff=0.0,
+                           with_j=True, with_k=True, device=None):
+    """Coordinate JVP of J/K at fixed density (the reference's
+    gradscf_direct_jk_geometry_jvp_cpu_v1, csrc/direct_jk_geometry.cc:8-99):
+    order 1, d/du (J, K), when ``vector`` is None; order 2, d^2/(du dv) (J, K),
+    with ``vector`` = v.  ``direction`` / ``vector`` are env-sized, nonzero only
+    at atm coordinate slots.  ``b200jk_direct_jk_geom_jvp``."""
+    plan, d, n, dev = _geometry_setup(atm, bas, env, density, cart, cutoff, with_j, with_k, device)
+    u, _ = _coordinate_rows(atm, direction, dev)
+    v = _coordinate_rows(atm, vector, dev)[0] if vector is not None else None
+    flat = d.reshape(-1, n * n).contiguous()
+    nb = flat.shape[0]
+    nops = int(bool(with_j)) + int(bool(with_k))
+    out = torch.empty((nops, nb, n * n), dtype=torch.float64, device=dev)
+    hermi = bool(torch.equal(flat.reshape(nb, n, n), flat.reshape(nb, n, n).transpose(-1, -2)))
+    with torch.cuda.device(dev):
+        st = _stream_handle()
+        _capi.check(_capi.lib().b200jk_direct_jk_geom_jvp(
+            plan._h, ctypes.c_void_p(flat.data_ptr()), nb, int(hermi), ctypes.c_void_p(u.data_ptr()),
+            ctypes.c_void_p(v.data_ptr()) if v is not None else None, int(bool(with_j)), int(bool(with_k)),
+            ctypes.c_void_p(out.data_ptr()), st))
+    plan.reduce_shards(out)
+    out = out.reshape(nops, *d.shape)
+    return (out[0] if with_j else torch.zeros_like(d), out[-1] if with_k else torch.zeros_like(d))
+
+
+def direct_jk_geometry_hvp(atm, bas, env, density, direction, cotangent, *, cart, cutoff=0.0,
+                           with_j=True, with_k=True, device=None):
+    """Order-2 coordinate VJP (the order-2 branch of the reference's
+    gradscf_direct_jk_geometry_vjp_cpu_v2): the env-sized coordinate gradient
+    of sum(Jbar * dJ/du + Kbar * dK/du), ``cotangent`` = (Jbar, Kbar) each
+    shaped like the density.  ``b200jk_direct_jk_geom_hvp``."""
+    plan, d, n, dev = _geometry_setup(atm, bas, env, density, cart, cutoff, with_j, with_k, device)
+    u, slots = _coordinate_rows(atm, direction, dev)
+    flat = d.reshape(-1, n * n).contiguous()
+    nb = flat.shape[0]
+    parts = []
+    jbar, kbar = cotangent
+    if with_j:
+        parts.append(torch.as_tensor(jbar, dtype=torch.float64, device=dev).reshape(nb, n * n))
+    if with_k:
+        parts.append(torch.as_tensor(kbar, dtype=torch.float64, device=dev).reshape(nb, n * n))
+    cot = torch.stack(parts).contiguous()
+    g = torch.empty((plan.natm[0], 3), dtype=torch.float64, device=dev)
+    with torch.cuda.device(dev):
+        st = _stream_handle()
+        _capi.check(_capi.lib().b200jk_direct_jk_geom_hvp(
+            plan._h, ctypes.c_void_p(flat.data_ptr()), nb, ctypes.c_void_p(u.data_ptr()),
+            ctypes.c_void_p(cot.data_ptr()), int(bool(with_j)), int(bool(with_k)),
+            ctypes.c_void_p(g.data_ptr()), st))
+    plan.reduce_shards(g)
+    out = np.zeros(np.asarray(env).shape[0])
+    np.add.at(out, slots.ravel(), g.cpu().numpy().ravel())
+    return out
+
+
 @dataclass(frozen=True)
 class IntegralPlan:
     """Static topology + table layout (plan.py:50-92)."""

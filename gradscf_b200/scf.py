@@ -202,6 +202,89 @@ def rhf_gradient(mol: Molecule, res: SCFResult):
     return out + nuclear_repulsion_gradient(mol.charges, mol.coords)
 
 
+def uhf_jk(mol: Molecule, density_a, density_b, *, with_k=True, precision="fp64",
+           fp32_cut=DEFAULT_FP32_CUT):
+    """Open-shell J/K as the reference's UKS caller builds them
+    (src/gradscf/scf/uks.py:255-265): one build of the stacked (D_a, D_b)
+    batch; J = J(D_a) + J(D_b), K_a = K(D_a), K_b = K(D_b).  Without K one
+    build of D_a + D_b.  Returns (D_tot, J, K_a, K_b)."""
+    d_tot = density_a + density_b
+    if not with_k:
+        j, _ = mol.plan.jk(d_tot, with_k=False, hermi=True, precision=precision, fp32_cut=fp32_cut)
+        z = torch.zeros_like(j)
+        return d_tot, j, z, z
+    j, k = mol.plan.jk(torch.stack((density_a, density_b)), hermi=True, precision=precision,
+                       fp32_cut=fp32_cut)
+    return d_tot, j.sum(0), k[0], k[1]
+
+
+@dataclass
+class UHFResult:
+    energy: float
+    converged: bool
+    cycles: int
+    density_a: torch.Tensor
+    density_b: torch.Tensor
+    energies: list = field(default_factory=list)
+
+
+def uhf(mol: Molecule, *, spin=0, conv_tol=1e-10, max_cycle=100, precision="fp64",
+        fp32_cut=DEFAULT_FP32_CUT, diis_space=8):
+    """Unrestricted Hartree-Fock on the batched (nb = 2) J/K build:
+    F_s = h + J - K_s, E = tr(D_tot h) + tr(D_tot J)/2 - (tr(D_a K_a) + tr(D_b K_b))/2
+    + E_nuc, with D_s = C_s,occ C_s,occ^T and spin = n_alpha - n_beta.
+    DIIS on the stacked alpha/beta commutators; core guess."""
+    dev = mol.device
+    s = mol.int1e("ovlp")
+    h = mol.int1e("kin") + mol.int1e("nuc")
+    w, v = torch.linalg.eigh(s)
+    x = v / torch.sqrt(w)
+    na = (mol.nelectron + spin) // 2
+    nb = mol.nelectron - na
+    if na - nb != spin or na < 0 or nb < 0:
+        raise ValueError("spin is incompatible with the electron count")
+    _, c = _solve(h, x)
+    da = c[:, :na] @ c[:, :na].T
+    db = c[:, :nb] @ c[:, :nb].T
+    hist_f, hist_e, energies = [], [], []
+    e_old = None
+    converged = False
+    cycle = 0
+    for cycle in range(1, max_cycle + 1):
+        dt, j, ka, kb = uhf_jk(mol, da, db, precision=precision, fp32_cut=fp32_cut)
+        fa, fb = h + j - ka, h + j - kb
+        energy = (torch.sum(dt * h) + 0.5 * torch.sum(dt * j)
+                  - 0.5 * (torch.sum(da * ka) + torch.sum(db * kb))).item() + mol.e_nuc
+        energies.append(energy)
+        err = torch.stack([x.T @ (fa @ da @ s - s @ da @ fa) @ x, x.T @ (fb @ db @ s - s @ db @ fb) @ x])
+        gnorm = torch.linalg.norm(err).item()
+        if e_old is not None and abs(energy - e_old) < conv_tol and gnorm < np.sqrt(conv_tol):
+            converged = True
+            break
+        hist_f.append(torch.stack([fa, fb]))
+        hist_e.append(err)
+        hist_f, hist_e = hist_f[-diis_space:], hist_e[-diis_space:]
+        f2 = torch.stack([fa, fb])
+        if len(hist_f) > 1:
+            m = len(hist_f)
+            bm = -torch.ones((m + 1, m + 1), dtype=torch.float64, device=dev)
+            bm[m, m] = 0.0
+            for i in range(m):
+                for k_ in range(i, m):
+                    bm[i, k_] = bm[k_, i] = torch.sum(hist_e[i] * hist_e[k_])
+            rhs = torch.zeros(m + 1, dtype=torch.float64, device=dev)
+            rhs[m] = -1.0
+            coef = torch.linalg.solve(bm, rhs)[:m]
+            f2 = sum(cf * fi for cf, fi in zip(coef, hist_f))
+        _, ca = _solve(f2[0], x)
+        _, cb = _solve(f2[1], x)
+        da = ca[:, :na] @ ca[:, :na].T
+        db = cb[:, :nb] @ cb[:, :nb].T
+        e_old = energy
+    return UHFResult(energy=energies[-1], converged=converged, cycles=cycle, density_a=da, density_b=db,
+                     energies=energies)
+
+
 class MoleculeBatch:
     """Independent molecules sharing one device plan (packed per-molecule blocks)."""
 

@@ -82,7 +82,7 @@ int b200jk_plan_class_stats(const b200jk_plan* plan, int64_t* quartets, int64_t*
  * rank `rank`'s items of every class pair (costs = primitive quartets), so
  * the J/K it returns is this rank's partial sum; the caller sums the ranks'
  * outputs (one all-reduce).  (0, 1) restores the whole build.  Graphs
- * created before the call keep the shard they captured. */
+ * created before the call must be recreated (their launch is refused). */
 int b200jk_partition_items(const int64_t* cost, int64_t n, int32_t world, int32_t* owner);
 int b200jk_plan_set_shard(b200jk_plan* plan, int32_t rank, int32_t world);
 
@@ -93,7 +93,7 @@ int b200jk_plan_set_shard(b200jk_plan* plan, int32_t rank, int32_t world);
  * 128 kets per work item (`reps` timed launches after one warm-up each) and
  * keeps the fastest.  chunks[55] (or NULL) receives the choice per class pair,
  * -1 where not tuned.  Synchronises `stream`; call it before creating graphs
- * (a graph keeps the work items it captured) and after set_shard. */
+ * (graphs created earlier must be recreated) and after set_shard. */
 int b200jk_plan_autotune(b200jk_plan* plan, const double* d_density, int32_t nb, int32_t hermi,
                          int32_t precision, double fp32_cut, int32_t reps, void* stream, int32_t* chunks);
 
@@ -157,8 +157,11 @@ int b200jk_direct_jk(b200jk_plan* plan, const double* d_density, int32_t nb, dou
  * until exit; a call needing more returns B200JK_INVALID_ARGUMENT with the
  * byte counts.  The plan must already exist (plan creation allocates).
  * All calls share the array: calls that overlap on the GPU race, so order
- * them on one stream.  The first call on a device looks up the array's
- * address with that device current -- make it before any stream capture. */
+ * them on one stream.  A call also uses the plan's small device state (row
+ * maxima, status word, FP32 boundaries), so it also races with any other
+ * build on the same plan that overlaps it on the GPU.  The first call on a
+ * device looks up the array's address with that device current -- make it
+ * before any stream capture.  The caller's current device is restored. */
 #define B200JK_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
 int b200jk_direct_jk_noalloc(b200jk_plan* plan, const double* d_density, int32_t nb, double* d_out,
                              int32_t with_j, int32_t with_k, int32_t hermi, int32_t precision,
@@ -168,9 +171,13 @@ int b200jk_direct_jk_noalloc(b200jk_plan* plan, const double* d_density, int32_t
  * class-pair kernel, finalisation) for fixed device buffers, replayed once
  * per SCF iteration: the reference runs one FFI call per iteration
  * (scf/rks.py:305-321); here the caller copies the next density into
- * d_density and launches the graph.  Creation runs one eager build (which
- * allocates the plan's scratch) before capturing.  The graph uses the plan's
- * scratch: do not run another build on the same plan concurrently. */
+ * d_density and launches the graph.  Creation allocates the graph's own
+ * scratch and runs one eager build before capturing, so later builds on the
+ * plan with more densities leave the graph valid.  The graph shares the
+ * plan's work items and small device state: do not run another build on the
+ * same plan concurrently, and after b200jk_plan_autotune or
+ * b200jk_plan_set_shard (which rebuild the work items) b200jk_graph_launch
+ * refuses with B200JK_INVALID_ARGUMENT -- destroy and recreate the graph. */
 typedef struct b200jk_graph b200jk_graph;
 int b200jk_graph_create(b200jk_plan* plan, const double* d_density, int32_t nb, double* d_out,
                         int32_t with_j, int32_t with_k, int32_t hermi, int32_t precision,
@@ -200,6 +207,27 @@ int b200jk_direct_jk_tables(const int32_t* atm, int32_t natm, const int32_t* bas
  * Unlike the reference (which demands cutoff 0), the plan's Schwarz cut is
  * applied; a plan built with cut 0 reproduces the reference exactly. */
 int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_t nb,
+                              const double* d_cot, int32_t with_j, int32_t with_k, double* d_grad,
+                              void* stream);
+
+/* Coordinate JVP of J/K (replaces gradscf_direct_jk_geometry_jvp_cpu_v1 with
+ * order 1 and 2, csrc/direct_jk_geometry.cc:8-99):
+ *   d_v == NULL : d_out = d/du (J, K)           (order 1)
+ *   d_v != NULL : d_out = d^2/(du dv) (J, K)    (order 2)
+ * at fixed density.  d_u, d_v: device, (sum_m natm_m, 3) coordinate directions
+ * per atm row (the coordinate slots of the reference's env-sized
+ * direction).  d_density / d_out / hermi as for b200jk_direct_jk.  The
+ * plan's Schwarz cut applies (cut 0 reproduces the reference). */
+int b200jk_direct_jk_geom_jvp(b200jk_plan* plan, const double* d_density, int32_t nb, int32_t hermi,
+                              const double* d_u, const double* d_v, int32_t with_j, int32_t with_k,
+                              double* d_out, void* stream);
+
+/* Order-2 coordinate VJP (Hessian-vector product; replaces the order-2 branch
+ * of gradscf_direct_jk_geometry_vjp_cpu_v2, csrc/direct_jk_geometry.cc:59-99
+ * over csrc/geometry_contraction.h:7-53): for cotangents (Jbar, Kbar) in d_cot
+ * (as for b200jk_direct_jk_geom_vjp) and a coordinate direction d_u,
+ *   d_grad[R] = d/dR sum(Jbar * dJ/du + Kbar * dK/du),  (sum_m natm_m, 3). */
+int b200jk_direct_jk_geom_hvp(b200jk_plan* plan, const double* d_density, int32_t nb, const double* d_u,
                               const double* d_cot, int32_t with_j, int32_t with_k, double* d_grad,
                               void* stream);
 

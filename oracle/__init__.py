@@ -154,3 +154,36 @@ def direct_jk_geometry_vjp(atm, bas, env, density, cotangent, *, cart, with_j=Tr
                                                len(env), _p(d), d.shape[0], n, _p(v), _p(out),
                                                int(cart), int(with_j), int(with_k), int(workers)))
     return out
+
+
+def direct_jk_geometry_product(atm, bas, env, density, direction, vector=None, *, order, cart,
+                               transpose=False, with_j=True, with_k=True, workers=1):
+    """The reference's geometry products of J/K (csrc/direct_jk_geometry.cc:8-99).
+
+    transpose=False (JVP): returns (J', K') with J' = d/du J (order 1) or
+    d^2/(du dv) J (order 2, ``vector`` = v, env-sized), same for K.
+    transpose=True (order 2 only): returns the env-sized coordinate gradient of
+    sum(Jbar * dJ/du + Kbar * dK/du), ``vector`` = (Jbar, Kbar) cotangents of
+    shape (with_j + with_k, nb, n, n)."""
+    atm, bas, env = _i32(atm), _i32(bas), _f64(env)
+    d = _f64(density)
+    shape = d.shape
+    n = shape[-1]
+    d = d.reshape(-1, n, n)
+    nb = d.shape[0]
+    u = _f64(direction)
+    nops = int(with_j) + int(with_k)
+    if transpose:
+        v = _f64(vector)
+        out = np.zeros(len(env))
+    else:
+        v = _f64(vector) if vector is not None else np.zeros(len(env))
+        out = np.zeros((nops, nb, n, n))
+    _check(lib().oracle_direct_jk_geometry_product(
+        _p(atm), len(atm), _p(bas), len(bas), _p(env), len(env), _p(d), nb, n, _p(u), _p(v), _p(out),
+        int(order), int(bool(transpose)), int(cart), int(with_j), int(with_k), int(workers)))
+    if transpose:
+        return out
+    j = out[0].reshape(shape) if with_j else np.zeros(shape)
+    k = out[-1].reshape(shape) if with_k else np.zeros(shape)
+    return j, k

@@ -15,6 +15,8 @@
  *   csrc/eri_geometry_entries.h:6-31   int2e_ip1 entries, four permutations
  *   csrc/direct_jk_geometry.cc:68-84   transposed (VJP) contraction
  *   csrc/direct_jk_geometry.cc:122-176 per-worker partial + fixed-order reduction
+ *   csrc/direct_jk_geometry.cc:8-99    geometry JVP (order 1, 2) and order-2 VJP
+ *   csrc/geometry_contraction.h:7-53   second-derivative ERI entries (ipip1, ipvip1, ip1ip2)
  * Workers are pthreads instead of XLA's pool; the partition of output
  * rows (direct J/K) and first shells (geometry VJP) is the reference's, so the
  * arithmetic order within each output element is the reference's too.
@@ -34,6 +36,12 @@ extern int int2e_sph(double *, int *, int *, int *, int, int *, int, double *, C
 extern int int2e_cart(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
 extern int int2e_ip1_sph(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
 extern int int2e_ip1_cart(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
+extern int int2e_ipip1_sph(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
+extern int int2e_ipip1_cart(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
+extern int int2e_ipvip1_sph(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
+extern int int2e_ipvip1_cart(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
+extern int int2e_ip1ip2_sph(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
+extern int int2e_ip1ip2_cart(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
 extern void int2e_optimizer(CINTOpt **, int *, int, int *, int, double *);
 extern void CINTdel_optimizer(CINTOpt **);
 extern int int1e_ovlp_sph(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
@@ -526,6 +534,182 @@ int oracle_direct_jk_geometry_vjp(const int32_t *atm, int natm, const int32_t *b
   memset(out, 0, sizeof(double) * (size_t)nenv);
   for (int worker = 0; worker < w; ++worker)
     for (int i = 0; i < nenv; ++i) out[i] += partials[(size_t)worker * nenv + i];
+  free(partials);
+  tables_free(&t);
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Geometry products of J/K (direct_jk_geometry.cc:8-99).
+ *   transpose = 0 (JVP): out (with_j+with_k, nb, n, n) = d/du J/K (order 1) or
+ *     d^2/du dv J/K (order 2); u = direction, v = vector (env-sized).
+ *   transpose = 1 (order-2 VJP): out (env-sized) = the coordinate gradient of
+ *     sum(Jbar * dJ/du + Kbar * dK/du); vector = (Jbar, Kbar) cotangents.
+ * Every ordered shell quartet (eri_window.h:91-105 without a window), per
+ * worker a range of first shells, partials summed in worker order. */
+typedef struct {
+  tables_t *t; int n, nb, with_j, with_k, transpose;
+  const double *dm, *u, *input; double *output;
+} geo_ctx_t;
+
+/* direct_jk_geometry.cc:65-81, the consume lambda */
+static void geo_consume(geo_ctx_t *g, int a, int b, int c, int d, int coordinate, double value) {
+  const int n = g->n;
+  const size_t nn = (size_t)n * n;
+  double sum = 0.;
+  for (int batch = 0; batch < g->nb; ++batch) {
+    const double *dmat = g->dm + (size_t)batch * nn;
+    if (g->transpose) {
+      if (g->with_j) sum += g->input[(size_t)batch * nn + (size_t)a * n + b] * dmat[(size_t)c * n + d];
+      if (g->with_k)
+        sum += g->input[(size_t)(g->with_j * g->nb + batch) * nn + (size_t)a * n + c] * dmat[(size_t)b * n + d];
+    } else {
+      if (g->with_j) g->output[(size_t)batch * nn + (size_t)a * n + b] += value * dmat[(size_t)c * n + d];
+      if (g->with_k)
+        g->output[(size_t)(g->with_j * g->nb + batch) * nn + (size_t)a * n + c] += value * dmat[(size_t)b * n + d];
+    }
+  }
+  if (g->transpose) g->output[coordinate] += value * sum;
+}
+
+/* direct_jk_geometry.cc:94-99: add(index, a, b, value) of the Hessian entries */
+static void geo_add2(geo_ctx_t *g, int a, int b, int c, int d, int pa, int pb, double value) {
+  geo_consume(g, a, b, c, d, pa, g->transpose ? value * g->u[pb] : value * g->u[pa] * g->input[pb]);
+}
+static void geo_cross(geo_ctx_t *g, int a, int b, int c, int d, int pa, int pb, double value) {
+  geo_add2(g, a, b, c, d, pa, pb, value);
+  geo_add2(g, a, b, c, d, pb, pa, value);
+}
+
+static int coord_ptr(const tables_t *t, int shell) {
+  return t->atm[t->bas[shell * BAS_SLOTS + ATOM_OF] * ATM_SLOTS + PTR_COORD];
+}
+
+/* order 1: eri_geometry_entries.h:6-31 entries, direct_jk_geometry.cc:84-88 */
+static void geometry_order1_range(geo_ctx_t *g, int cart, int fs, int ls) {
+  tables_t *t = g->t;
+  intor_t ip = cart ? int2e_ip1_cart : int2e_ip1_sph;
+  scratch_t s = {0};
+  for (int i = fs; i < ls; ++i)
+    for (int j = 0; j < t->nbas; ++j)
+      for (int k = 0; k < t->nbas; ++k)
+        for (int l = 0; l < t->nbas; ++l) {
+          int sh[4] = {i, j, k, l};
+          const int di = t->ao[i + 1] - t->ao[i], dj = t->ao[j + 1] - t->ao[j];
+          const int dk = t->ao[k + 1] - t->ao[k], dl = t->ao[l + 1] - t->ao[l];
+          const size_t size = (size_t)di * dj * dk * dl;
+          eval_block(t, ip, NULL, sh, 3 * size, &s);
+          const int coord0 = coord_ptr(t, i);
+          for (int x = 0; x < 3; ++x)
+            for (int w = 0; w < dl; ++w)
+              for (int r = 0; r < dk; ++r)
+                for (int q = 0; q < dj; ++q)
+                  for (int p = 0; p < di; ++p) {
+                    const double value = -s.data[x * size + (((size_t)w * dk + r) * dj + q) * di + p];
+                    const int a = t->ao[i] + p, b = t->ao[j] + q, c = t->ao[k] + r, d = t->ao[l] + w;
+                    const int perm[4][4] = {{a, b, c, d}, {b, a, c, d}, {c, d, a, b}, {c, d, b, a}};
+                    for (int e = 0; e < 4; ++e)
+                      geo_consume(g, perm[e][0], perm[e][1], perm[e][2], perm[e][3], coord0 + x,
+                                  g->transpose ? value : value * g->u[coord0 + x]);
+                  }
+        }
+  free(s.data); free(s.cache);
+}
+
+/* order 2: geometry_contraction.h:24-53 (op == 4) */
+static void geometry_order2_range(geo_ctx_t *g, int cart, int fs, int ls) {
+  tables_t *t = g->t;
+  intor_t kernels[3] = {cart ? int2e_ipip1_cart : int2e_ipip1_sph, cart ? int2e_ipvip1_cart : int2e_ipvip1_sph,
+                        cart ? int2e_ip1ip2_cart : int2e_ip1ip2_sph};
+  scratch_t s = {0};
+  for (int i = fs; i < ls; ++i)
+    for (int j = 0; j < t->nbas; ++j)
+      for (int k = 0; k < t->nbas; ++k)
+        for (int l = 0; l < t->nbas; ++l) {
+          int sh[4] = {i, j, k, l};
+          const int di = t->ao[i + 1] - t->ao[i], dj = t->ao[j + 1] - t->ao[j];
+          const int dk = t->ao[k + 1] - t->ao[k], dl = t->ao[l + 1] - t->ao[l];
+          const size_t size = (size_t)di * dj * dk * dl;
+          for (int kind = 0; kind < 3; ++kind) {
+            eval_block(t, kernels[kind], NULL, sh, 9 * size, &s);
+            for (int x = 0; x < 3; ++x)
+              for (int y = 0; y < 3; ++y)
+                for (int w = 0; w < dl; ++w)
+                  for (int r = 0; r < dk; ++r)
+                    for (int q = 0; q < dj; ++q)
+                      for (int p = 0; p < di; ++p) {
+                        const double value = s.data[(x * 3 + y) * size + (((size_t)w * dk + r) * dj + q) * di + p];
+                        const int a = t->ao[i] + p, b = t->ao[j] + q, c = t->ao[k] + r, d = t->ao[l] + w;
+                        const int px = coord_ptr(t, i) + x;
+                        if (kind == 0) {
+                          const int py = coord_ptr(t, i) + y;
+                          geo_add2(g, a, b, c, d, px, py, value); geo_add2(g, b, a, c, d, px, py, value);
+                          geo_add2(g, c, d, a, b, px, py, value); geo_add2(g, c, d, b, a, px, py, value);
+                        } else if (kind == 1) {
+                          const int py = coord_ptr(t, j) + y;
+                          geo_cross(g, a, b, c, d, px, py, value);
+                          geo_cross(g, c, d, a, b, px, py, value);
+                        } else {
+                          const int py = coord_ptr(t, k) + y;
+                          geo_cross(g, a, b, c, d, px, py, value); geo_cross(g, b, a, c, d, px, py, value);
+                          geo_cross(g, a, b, d, c, px, py, value); geo_cross(g, b, a, d, c, px, py, value);
+                        }
+                      }
+          }
+        }
+  free(s.data); free(s.cache);
+}
+
+typedef struct {
+  const int32_t *atm; int natm; const int32_t *bas; int nbas; const double *env; int nenv;
+  int cart, order, nb, with_j, with_k, transpose; const double *dm, *u, *input;
+  int fs, ls; double *output;
+} geo_task_t;
+
+static void *geo_task_run(void *arg) {
+  geo_task_t *k = (geo_task_t *)arg;
+  tables_t local;
+  tables_init(&local, k->atm, k->natm, k->bas, k->nbas, k->env, k->nenv, k->cart);
+  geo_ctx_t g = {&local, local.n, k->nb, k->with_j, k->with_k, k->transpose, k->dm, k->u, k->input, k->output};
+  if (k->order == 1) geometry_order1_range(&g, k->cart, k->fs, k->ls);
+  else geometry_order2_range(&g, k->cart, k->fs, k->ls);
+  tables_free(&local);
+  return NULL;
+}
+
+int oracle_direct_jk_geometry_product(const int32_t *atm, int natm, const int32_t *bas, int nbas,
+                                      const double *env, int nenv, const double *density, int nb,
+                                      int n, const double *direction, const double *vector,
+                                      double *out, int order, int transpose, int cart, int with_j,
+                                      int with_k, int workers) {
+  if (workers < 1) return fail("Direct J/K geometry workers must be positive");
+  if ((order != 1 && order != 2) || (with_j != 0 && with_j != 1) || (with_k != 0 && with_k != 1) ||
+      !(with_j || with_k))
+    return fail("Invalid direct J/K geometry product");
+  if (transpose && order != 2) return fail("order-1 VJP: use oracle_direct_jk_geometry_vjp");
+  tables_t t;
+  if (tables_init(&t, atm, natm, bas, nbas, env, nenv, cart)) { tables_free(&t); return 1; }
+  if (n != t.n) { tables_free(&t); return fail("Direct J/K geometry density shape mismatch"); }
+  const int nops = with_j + with_k;
+  const size_t osize = transpose ? (size_t)nenv : (size_t)nops * nb * n * n;
+  int w = workers < host_threads() ? workers : host_threads();
+  if (w > t.nbas) w = t.nbas;
+  double *partials = calloc((size_t)w * osize, sizeof(double));
+  geo_task_t *tasks = calloc((size_t)w, sizeof(geo_task_t));
+  pthread_t *threads = calloc((size_t)w, sizeof(pthread_t));
+  for (int worker = 0; worker < w; ++worker) {
+    geo_task_t task = {atm, natm, bas, nbas, env, nenv, cart, order, nb, with_j, with_k, transpose,
+                       density, direction, vector, worker * t.nbas / w, (worker + 1) * t.nbas / w,
+                       partials + (size_t)worker * osize};
+    tasks[worker] = task;
+  }
+  for (int worker = 1; worker < w; ++worker) pthread_create(&threads[worker], NULL, geo_task_run, &tasks[worker]);
+  geo_task_run(&tasks[0]);
+  for (int worker = 1; worker < w; ++worker) pthread_join(threads[worker], NULL);
+  free(tasks); free(threads);
+  memset(out, 0, sizeof(double) * osize);
+  for (int worker = 0; worker < w; ++worker)
+    for (size_t i = 0; i < osize; ++i) out[i] += partials[(size_t)worker * osize + i];
   free(partials);
   tables_free(&t);
   return 0;

@@ -111,3 +111,50 @@ def rhf_gradient(atm, bas, env, result, charges, coords, shell_atoms, *, cart, w
                 r = coords[i] - coords[j]
                 grad[i] -= charges[i] * charges[j] * r / np.linalg.norm(r) ** 3
     return grad
+
+
+def uhf(atm, bas, env, nalpha, nbeta, charges, coords, *, cart, conv_tol=1e-12, max_cycle=100,
+        workers=8):
+    """Plain DIIS UHF on stacked (D_a, D_b) direct J/K builds, as the
+    reference's UKS caller builds them (src/gradscf/scf/uks.py:255-265):
+    J = J(D_a) + J(D_b), K_s = K(D_s), F_s = h + J - K_s,
+    E = tr(D_tot h) + tr(D_tot J)/2 - (tr(D_a K_a) + tr(D_b K_b))/2 + E_nuc."""
+    s = int1e(atm, bas, env, "ovlp", cart=cart)
+    h = int1e(atm, bas, env, "kin", cart=cart) + int1e(atm, bas, env, "nuc", cart=cart)
+    e_nuc = _nuclear_repulsion(charges, coords)
+    w, v = np.linalg.eigh(s)
+    x = v / np.sqrt(w)
+
+    def solve(f):
+        e, c = np.linalg.eigh(x.T @ f @ x)
+        return e, x @ c
+
+    _, c = solve(h)
+    da, db = c[:, :nalpha] @ c[:, :nalpha].T, c[:, :nbeta] @ c[:, :nbeta].T
+    hist_f, hist_e = [], []
+    e_old = None
+    for cycle in range(max_cycle):
+        j, k = direct_jk(atm, bas, env, np.stack([da, db]), cart=cart, workers=workers)
+        jt = j.sum(0)
+        fa, fb = h + jt - k[0], h + jt - k[1]
+        dt = da + db
+        energy = np.sum(dt * h) + 0.5 * np.sum(dt * jt) - 0.5 * (np.sum(da * k[0]) + np.sum(db * k[1])) + e_nuc
+        err = np.stack([x.T @ (fa @ da @ s - s @ da @ fa) @ x, x.T @ (fb @ db @ s - s @ db @ fb) @ x])
+        if e_old is not None and abs(energy - e_old) < conv_tol and np.linalg.norm(err) < np.sqrt(conv_tol):
+            return dict(energy=energy, density_a=da, density_b=db, cycles=cycle + 1)
+        hist_f.append(np.stack([fa, fb])); hist_e.append(err)
+        hist_f, hist_e = hist_f[-8:], hist_e[-8:]
+        f2 = np.stack([fa, fb])
+        if len(hist_f) > 1:
+            m = len(hist_f)
+            bm = -np.ones((m + 1, m + 1)); bm[m, m] = 0.0
+            for i in range(m):
+                for jj in range(m):
+                    bm[i, jj] = np.sum(hist_e[i] * hist_e[jj])
+            rhs = np.zeros(m + 1); rhs[m] = -1.0
+            coef = np.linalg.solve(bm, rhs)[:m]
+            f2 = sum(cf * fi for cf, fi in zip(coef, hist_f))
+        _, ca = solve(f2[0]); _, cb = solve(f2[1])
+        da, db = ca[:, :nalpha] @ ca[:, :nalpha].T, cb[:, :nbeta] @ cb[:, :nbeta].T
+        e_old = energy
+    return dict(energy=energy, density_a=da, density_b=db, cycles=max_cycle)

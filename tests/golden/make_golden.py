@@ -10,7 +10,7 @@
   hand-written general-contraction basis with a d shell (both cart and sph),
   seeded nonsymmetric densities (default_rng(801), nvec 4), einsum J/K.
 
-Usage: python tests/golden/make_golden.py [/root/reference]
+Usage: python tests/golden/make_golden.py <reference checkout>  (or GRADSCF_REFERENCE=<checkout>)
 """
 import json
 import sys
@@ -57,4 +57,8 @@ def main(reference):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GRADSCF_REFERENCE")
+    if not root:
+        sys.exit("give the reference checkout as the argument or in GRADSCF_REFERENCE")
+    main(root)

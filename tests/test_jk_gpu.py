@@ -329,3 +329,31 @@ def test_repeated_builds_agree_to_rounding():
     for _ in range(3):
         again = plan.jk_packed(d, hermi=0)
         assert (again - first).abs().max().item() <= 1e-12 * max(1.0, first.abs().max().item())
+
+
+def test_graph_survives_scratch_growth_and_refuses_stale_work_items():
+    # a graph owns its scratch: a later build with more densities (which grows
+    # the plan's scratch) leaves it valid; autotune rebuilds the work items,
+    # after which the graph's launch is refused instead of replaying stale items
+    from gradscf_b200 import workloads as W
+    top, par, sa, atm, bas, env = tables(W.water_cluster(2, 1), "cc-pvdz", False)
+    plan = J.DirectJKPlan([(atm, bas, env)], cart=False, cutoff=1e-12)
+    n = plan.nao[0]
+    d = psd_density(n, 10, 21)
+    j0, k0 = oracle.direct_jk(atm, bas, env, d, cart=False, cutoff=1e-12, workers=8)
+    g = J.JKGraph(plan, 1, hermi=1)
+    big = torch.as_tensor(np.stack([psd_density(n, 10, 22 + i) for i in range(3)]).reshape(3, -1),
+                          device="cuda")
+    plan.jk_packed(big, hermi=1)
+    for _ in range(2):
+        out = g.run(torch.as_tensor(d.reshape(1, -1), device="cuda")).cpu().numpy()
+        assert np.abs(out[0, 0].reshape(n, n) - j0).max() < 1e-10
+        assert np.abs(out[1, 0].reshape(n, n) - k0).max() < 1e-10
+    plan.autotune(big[:1], precision="fp64", reps=1)
+    with pytest.raises(_capi.InvalidArgument, match="recreate|create a new one"):
+        g.launch()
+    g.close()
+    g = J.JKGraph(plan, 1, hermi=1)
+    out = g.run(torch.as_tensor(d.reshape(1, -1), device="cuda")).cpu().numpy()
+    assert np.abs(out[1, 0].reshape(n, n) - k0).max() < 1e-10
+    g.close()

@@ -82,3 +82,42 @@ def test_invalid_inputs_raise():
     bad = bas.copy(); bad[0, 1] = 13
     with pytest.raises(oracle.OracleError, match="unsupported"):
         oracle.direct_jk(atm, bad, env, np.eye(2), cart=True)
+
+
+@pytest.mark.parametrize("cart", [True, False], ids=["cart", "sph"])
+def test_geometry_products_restatement_vs_finite_differences(cart):
+    # the reference's geometry-response fixture: H2 at (0,0,0), (.2,-.1,.8)
+    # Angstrom, 3-21G, nonsymmetric densities from seed 932
+    # (tests/integrals/test_direct_geometry_response.py:14-24); plus water
+    # 6-31G* for d shells.  Order 1 = d/du J/K, order 2 = d/dv of order 1,
+    # the order-2 VJP = the gradient of <cot, order 1>, checked by central
+    # differences of the oracle itself (step 1e-4 Bohr).
+    for atom, basis in (("H 0 0 0; H .2 -.1 .8", "3-21g"),
+                        ("O 0 0 0; H 0 0.7572 0.5865; H 0 -0.7572 0.5865", "6-31g*")):
+        top, par, _ = B.prepare_basis(atom, basis, cart=cart)
+        atm, bas, env = B.pack(top, par)
+        n = top.nao
+        rng = np.random.default_rng(932)
+        d = rng.normal(size=(2, n, n))
+        slots = (atm[:, 1][:, None] + np.arange(3)[None, :]).ravel()
+        u = np.zeros(len(env))
+        v = np.zeros(len(env))
+        u[slots] = rng.normal(size=slots.size) * .17
+        v[slots] = rng.normal(size=slots.size) * .11
+        h = 1e-4
+        jk = lambda e: oracle.direct_jk(atm, bas, e, d, cart=cart, workers=4)  # noqa: E731
+        jvp1 = lambda e: oracle.direct_jk_geometry_product(atm, bas, e, d, u, order=1, cart=cart,  # noqa: E731
+                                                            workers=4)
+        j1, k1 = jvp1(env)
+        (jp, kp), (jm, km) = jk(env + h * u), jk(env - h * u)
+        np.testing.assert_allclose(j1, (jp - jm) / (2 * h), atol=2e-7, rtol=3e-7)
+        np.testing.assert_allclose(k1, (kp - km) / (2 * h), atol=2e-7, rtol=3e-7)
+        j2, k2 = oracle.direct_jk_geometry_product(atm, bas, env, d, u, v, order=2, cart=cart, workers=4)
+        (jp, kp), (jm, km) = jvp1(env + h * v), jvp1(env - h * v)
+        np.testing.assert_allclose(j2, (jp - jm) / (2 * h), atol=2e-7, rtol=3e-7)
+        np.testing.assert_allclose(k2, (kp - km) / (2 * h), atol=2e-7, rtol=3e-7)
+        cot = np.stack([np.cos(d), np.sin(d)])
+        g = oracle.direct_jk_geometry_product(atm, bas, env, d, u, cot, order=2, cart=cart,
+                                              transpose=True, workers=4)
+        assert abs(g @ v - (np.sum(cot[0] * j2) + np.sum(cot[1] * k2))) < 1e-10
+        assert np.all(g[np.setdiff1d(np.arange(len(env)), slots)] == 0.0)

@@ -97,3 +97,24 @@ def test_batched_rhf_matches_single_molecule_rhf(precision, use_graph):
         ref = S.rhf(mol, conv_tol=1e-10, precision=precision)
         assert abs(en[m] - ref.energy) < 1e-8, (m, en[m], ref.energy)
         assert ds[m].shape == (mol.nao, mol.nao)
+
+
+def test_uhf_doublet_on_stacked_alpha_beta_builds_vs_oracle():
+    # the reference's UKS caller (scf/uks.py:255-265) stacks (D_a, D_b) into
+    # one nb = 2 direct J/K call; here the GPU UHF of the water cation
+    # (doublet, cc-pVDZ) against the oracle's UHF on the same stacked builds
+    from oracle import scf as OS
+    mol = S.Molecule(WATER, "cc-pvdz", cart=False, schwarz_cut=0.0, charge=1)
+    res = S.uhf(mol, spin=1, conv_tol=1e-11)
+    assert res.converged
+    na = (mol.nelectron + 1) // 2
+    ref = OS.uhf(mol.atm, mol.bas, mol.env, na, mol.nelectron - na, mol.charges, mol.coords, cart=False,
+                 conv_tol=1e-12)
+    assert abs(res.energy - ref["energy"]) < 1e-8
+    # one stacked build against the oracle's at the converged densities
+    da, db = res.density_a, res.density_b
+    dt, j, ka, kb = S.uhf_jk(mol, da, db)
+    j0, k0 = oracle.direct_jk(mol.atm, mol.bas, mol.env, np.stack([da.cpu().numpy(), db.cpu().numpy()]),
+                              cart=False, workers=8)
+    assert np.abs(j.cpu().numpy() - j0.sum(0)).max() < 1e-10
+    assert np.abs(ka.cpu().numpy() - k0[0]).max() < 1e-10 and np.abs(kb.cpu().numpy() - k0[1]).max() < 1e-10
