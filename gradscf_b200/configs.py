@@ -202,27 +202,55 @@ def run_prof(case="jk", nwater=8, basis="cc-pvdz", seed=1):
     plan = J.DirectJKPlan([(atm, bas, env)], cart=False, cutoff=1e-12)
     d = torch.as_tensor(W.psd_density(n, 5 * nwater, 0), device=plan.device).reshape(1, -1)
     out = {"config": "prof", "case": case, "system": f"(H2O){nwater} {basis}", "nao": n}
+    import ctypes
+    from . import _capi
+    lib = _capi.lib()
+    nc = _capi.NCLASS
     for precision in ("fp64", "split"):
+        plan.jk_packed(d, hermi=1, precision=precision)   # first use: kernel attributes, module load
         e0, e1 = _events()
         e0.record()
         plan.jk_packed(d, hermi=1, precision=precision)
         e1.record()
         torch.cuda.synchronize()
         out[f"{precision}_ms"] = e0.elapsed_time(e1)
+        # per-class launch times of one more build (serial launches, CUDA events)
+        lib.b200jk_plan_set_profiling(plan._h, 1)
+        plan.jk_packed(d, hermi=1, precision=precision)
+        ms64 = (ctypes.c_double * nc)(); ms32 = (ctypes.c_double * nc)(); nl = (ctypes.c_int32 * nc)()
+        _capi.check(lib.b200jk_plan_profile(plan._h, ms64, ms32, nl))
+        lib.b200jk_plan_set_profiling(plan._h, 0)
+        cls = {}
+        for c in range(nc):
+            for tag, arr in (("f64", ms64), ("f32", ms32)):
+                if arr[c] > 0:
+                    cls["({}{}|{}{}){}".format(*_capi.QUARTET_CLASSES[c], tag)] = round(arr[c], 4)
+        out[f"{precision}_class_ms"] = cls
     if case == "grad":
-        import ctypes
-        from . import _capi
         g = torch.zeros((plan.natm[0], 3), dtype=torch.float64, device=plan.device)
         cot = torch.stack([d / 2.0, -d / 4.0]).contiguous()
         st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+        def vjp():
+            _capi.check(lib.b200jk_direct_jk_geom_vjp(plan._h, ctypes.c_void_p(d.data_ptr()), 1,
+                                                      ctypes.c_void_p(cot.data_ptr()), 1, 1,
+                                                      ctypes.c_void_p(g.data_ptr()), st))
+        vjp()   # first use
         e0, e1 = _events()
         e0.record()
-        _capi.check(_capi.lib().b200jk_direct_jk_geom_vjp(plan._h, ctypes.c_void_p(d.data_ptr()), 1,
-                                                          ctypes.c_void_p(cot.data_ptr()), 1, 1,
-                                                          ctypes.c_void_p(g.data_ptr()), st))
+        vjp()
         e1.record()
         torch.cuda.synchronize()
         out["vjp_ms"] = e0.elapsed_time(e1)
+        # per-class launch times of one more VJP (serial launches, CUDA events)
+        nc = _capi.NCLASS
+        lib.b200jk_plan_set_profiling(plan._h, 1)
+        vjp()
+        ms64 = (ctypes.c_double * nc)(); ms32 = (ctypes.c_double * nc)(); nl = (ctypes.c_int32 * nc)()
+        _capi.check(lib.b200jk_plan_profile(plan._h, ms64, ms32, nl))
+        lib.b200jk_plan_set_profiling(plan._h, 0)
+        out["vjp_class_ms"] = {"({}{}|{}{})".format(*_capi.QUARTET_CLASSES[c]): round(ms64[c], 4)
+                               for c in range(nc) if ms64[c] > 0}
     plan.close()
     return out
 

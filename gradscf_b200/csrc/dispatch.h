@@ -104,6 +104,24 @@ B200JK_FOR_EACH_CLASS_PAIR(B200JK_DECLARE_REG)
 
 const DispatchTable& dispatch();
 
+// Blocks of a persistent launch: the kernel's resident blocks per SM times
+// the SM count of the current device (looked up once per device).
+template <typename Kernel>
+inline int persistent_blocks(Kernel* kernel, int threads, size_t smem, std::atomic<int>* cache /* [64] */) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  if (dev < 64) {
+    const int v = cache[dev].load(std::memory_order_acquire);
+    if (v > 0) return v;
+  }
+  int per_sm = 1, sms = 148;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int v = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  if (dev < 64) cache[dev].store(v, std::memory_order_release);
+  return v;
+}
+
 // Dynamic shared memory above 48 KB is an opt-in attribute of each kernel in
 // each device's context: set it on the current device the first time a
 // kernel is launched there (bit d of `done` marks device d; any thread).

@@ -740,6 +740,20 @@ static void fill_group(GroupWork& G, const ClassList& X, const ClassList& Y, boo
       }
     }
   }
+  // longest first: the persistent kernels take items in list order
+  {
+    std::vector<int> ord(G.all_items.size());
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return G.item_cost[a] > G.item_cost[b]; });
+    std::vector<int4> items(ord.size());
+    std::vector<int64_t> cost(ord.size());
+    for (size_t i = 0; i < ord.size(); ++i) {
+      items[i] = G.all_items[ord[i]];
+      cost[i] = G.item_cost[ord[i]];
+    }
+    G.all_items = std::move(items);
+    G.item_cost = std::move(cost);
+  }
   G.nwork = (int)G.all_items.size();
   CUDA_OK(G.work.ensure(std::max<size_t>(G.all_items.size(), 1) * sizeof(int4)));
   if (!G.all_items.empty())
@@ -1405,6 +1419,7 @@ static Plan* build_plan(const b200jk_molecule* mols, int nmol, int cart, double 
     }
     p.quartets = total;
   }
+  CUDA_OK(p.d_queue.ensure(kQueueSlots * sizeof(int)));
   for (int i = 0; i < kAuxStreams; ++i) {
     CUDA_OK(cudaStreamCreateWithFlags(&p.aux[i], cudaStreamNonBlocking));
     CUDA_OK(cudaEventCreateWithFlags(&p.join_ev[i], cudaEventDisableTiming));
@@ -1508,6 +1523,12 @@ static void launch_units(Plan& p, ClassPairWork& W, JKArgs a, int precision, cud
     if (!l64 || !l32) throw Failure{B200JK_INTERNAL, "no kernel for this contraction grouping"};
     auto launch = [&](int mode, bool fp32) {
       a.split_mode = mode;
+      if (u.grp) {
+        // a zeroed work-queue counter of its own (slots cycle over the plan's pool)
+        int* q = p.d_queue.as<int>() + (p.next_queue++ % kQueueSlots);
+        CUDA_OK(cudaMemsetAsync(q, 0, sizeof(int), st));
+        a.queue = q;
+      }
       ProfileEvent ev{cls, fp32 ? 1 : 0, nullptr, nullptr};
       if (p.profiling && allow_profiling) {
         CUDA_OK(cudaEventCreate(&ev.start));

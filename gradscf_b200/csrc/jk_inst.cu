@@ -1,6 +1,8 @@
 // Instantiates the J/K kernels of one class pair (BRA_CLASS >= KET_CLASS,
 // compiled once per pair so the classes build in parallel) and registers
 // their launchers in the dispatch table.
+#include <algorithm>
+
 #include "dispatch.h"
 #include "grad_kernels.cuh"
 #include "jk_kernels.cuh"
@@ -84,18 +86,25 @@ int launch_store(const JKArgs& args, int cart, int layout, double* out, long lon
   return (int)cudaGetLastError();
 }
 
+// Persistent launches of the bra-group kernels: at most one wave of resident
+// blocks; their warps take items from args.queue (zeroed by the caller).
 template <int LA, int LB, int LC, int LD, typename R>
 int launch_grp(const JKArgs& args, cudaStream_t stream) {
   if (args.nwork <= 0) return 0;
-  jk_grp_kernel<LA, LB, LC, LD, R><<<(args.nwork + kRegWarps - 1) / kRegWarps, 32 * kRegWarps, 0, stream>>>(args);
+  static std::atomic<int> resident[64];
+  const int wave = persistent_blocks(jk_grp_kernel<LA, LB, LC, LD, R>, 32 * kRegWarps, 0, resident);
+  const int blocks = std::min((args.nwork + kRegWarps - 1) / kRegWarps, wave);
+  jk_grp_kernel<LA, LB, LC, LD, R><<<blocks, 32 * kRegWarps, 0, stream>>>(args);
   return (int)cudaGetLastError();
 }
 
 template <int LA, int LB, int LC, int LD, typename R, int GB, int GK>
 int launch_grp_gen(const JKArgs& args, cudaStream_t stream) {
   if (args.nwork <= 0) return 0;
-  jk_grp_gen_kernel<LA, LB, LC, LD, R, GB, GK>
-      <<<(args.nwork + kRegWarps - 1) / kRegWarps, 32 * kRegWarps, 0, stream>>>(args);
+  static std::atomic<int> resident[64];
+  const int wave = persistent_blocks(jk_grp_gen_kernel<LA, LB, LC, LD, R, GB, GK>, 32 * kRegWarps, 0, resident);
+  const int blocks = std::min((args.nwork + kRegWarps - 1) / kRegWarps, wave);
+  jk_grp_gen_kernel<LA, LB, LC, LD, R, GB, GK><<<blocks, 32 * kRegWarps, 0, stream>>>(args);
   return (int)cudaGetLastError();
 }
 

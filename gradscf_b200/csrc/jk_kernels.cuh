@@ -67,6 +67,7 @@ struct JKArgs {
   const double* ket_q;
   const double* item_m;
   double cutoff, fp32_cut;
+  int* queue;                // persistent kernels: the launch's item counter (zeroed before it)
   const int* ws_atm;         // atm row of each work shell's centre
   double* grad;              // (atm rows, 3)
   // coordinate JVP / Hessian-vector products: directions, (atm rows, 3)
@@ -762,8 +763,13 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
     __syncthreads();
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int item = blockIdx.x * kRegWarps + warp;
-  if (item >= args.nwork) return;
+  // persistent warps: items are taken from the launch's queue in list order
+  // (the host sorts them by cost, longest first)
+  for (;;) {
+  int item = 0;
+  if (lane == 0) item = atomicAdd(args.queue, 1);
+  item = __shfl_sync(0xffffffffu, item, 0);
+  if (item >= args.nwork) break;
   const int4 w = args.work[item];  // (bra-order begin, bra count, ket begin, ket end)
   const double qm = args.split_mode != 0 ? args.item_m[item] : 0.0;
   const double cut = args.cutoff;
@@ -933,6 +939,7 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
       }
     }
   }
+  }  // items
 }
 
 // ---------------------------------------------------------------------------
@@ -1184,8 +1191,13 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
     __syncthreads();
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int item = blockIdx.x * kRegWarps + warp;
-  if (item >= args.nwork) return;
+  // persistent warps: items are taken from the launch's queue in list order
+  // (the host sorts them by cost, longest first)
+  for (;;) {
+  int item = 0;
+  if (lane == 0) item = atomicAdd(args.queue, 1);
+  item = __shfl_sync(0xffffffffu, item, 0);
+  if (item >= args.nwork) break;
   const int4 w = args.work[item];  // (bra-order begin, bra count, ket begin, ket end)
   const double qm = args.split_mode != 0 ? args.item_m[item] : 0.0;
   const double cut = args.cutoff;
@@ -1406,6 +1418,7 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
       }
     }
   }
+  }  // items
 }
 
 // ---------------------------------------------------------------------------

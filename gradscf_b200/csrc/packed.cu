@@ -1,10 +1,10 @@
 // J/K from packed ERIs (the reference's PackedJK, csrc/packed_jk.cc:6-80):
 // s8 storage (np(np+1)/2 values, np = n(n+1)/2) or s4 (np x np), any real
 // density batch (nonsymmetric allowed), output (with_j + with_k, nb, n, n)
-// overwritten.  One warp per pair row ab: the row's contributions to
-// J[a][b] are warp-reduced, every other element is an atomic add.
+// overwritten.  One warp per pair row ab (packed_jk_kernel below).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <stdexcept>
 #include <string>
@@ -24,56 +24,121 @@ __device__ __forceinline__ void unpair(long long pr, int& i, int& j) {
   j = (int)(pr - r * (r + 1) / 2);
 }
 
+// One block (one warp) per pair row ab = (a, b), a >= b: the row's
+// elements (ab|cd), cd <= ab, are read once, contiguously, for every
+// density.  Its exchange contributions all land in rows a, b and columns
+// a, b of K: they are summed in shared memory (K[a][.], K[b][.], K[.][a],
+// K[.][b], one column per density) and added to K once per row.  The loop
+// runs over c with the lanes on d, so terms indexed by d go to distinct
+// shared addresses and terms indexed by c are warp-reduced first.  J[a][b]
+// is warp-reduced; J[c][d] (cd < ab) takes one add per element into the
+// pair-packed accumulator `jp`, unfolded by packed_j_out_kernel.
 __global__ void packed_jk_kernel(const double* __restrict__ eri, int layout, int n, long long np,
                                  const double* __restrict__ dens, int nb, double* __restrict__ out,
-                                 int with_j, int with_k) {
-  const long long ab = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
+                                 double* __restrict__ jp, int with_j, int with_k) {
+  extern __shared__ double sk[];  // [nb][4][n]: K[a][x], K[b][x], K[x][a], K[x][b]
+  const long long ab = blockIdx.x;
+  const int lane = threadIdx.x;
   if (ab >= np) return;
   int a, b;
   unpair(ab, a, b);
   const long long nn = (long long)n * n;
   const double* row = layout == 1 ? eri + ab * (ab + 1) / 2 : eri + ab * np;
-  for (int e = 0; e < nb; ++e) {
-    const double* D = dens + e * nn;
-    double* J = with_j ? out + e * nn : nullptr;
-    double* K = with_k ? out + ((long long)with_j * nb + e) * nn : nullptr;
-    double jab = 0.0;
-    const double dab = D[(long long)a * n + b] + (a != b ? D[(long long)b * n + a] : 0.0);
-    for (long long cd = lane; cd <= ab; cd += 32) {
-      int c, d;
-      unpair(cd, c, d);
-      const double v = row[cd];
-      if (v == 0.0) continue;
-      if (J) {
-        jab += v * (D[(long long)c * n + d] + (c != d ? D[(long long)d * n + c] : 0.0));
-        if (ab != cd) {
-          const double jcd = v * dab;
-          atomicAdd(J + (long long)c * n + d, jcd);
-          if (c != d) atomicAdd(J + (long long)d * n + c, jcd);
+  if (with_k)
+    for (int i = lane; i < 4 * n * nb; i += 32) sk[i] = 0.0;
+  __syncwarp();
+  double jab[4] = {0.0, 0.0, 0.0, 0.0};   // densities in chunks of 4 (J[a][b])
+  for (int e0 = 0; e0 < nb; e0 += 4) {
+    const int ne = min(4, nb - e0);
+    for (int c = 0; c <= a; ++c) {
+      const int dmax = c == a ? b : c;
+      double rc[4][4];   // [density][K[a][c], K[b][c], K[c][a], K[c][b]] for this c
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) rc[x][y] = 0.0;
+      for (int d = lane; d <= dmax; d += 32) {
+        const long long cd = (long long)c * (c + 1) / 2 + d;
+        const double v = row[cd];
+        if (v == 0.0) continue;
+        const bool offd = c != d, offab = a != b, notdiag = ab != cd;
+        for (int q = 0; q < ne; ++q) {
+          const int e = e0 + q;
+          const double* D = dens + e * nn;
+          if (with_j) {
+            jab[q] += v * (D[(long long)c * n + d] + (offd ? D[(long long)d * n + c] : 0.0));
+            if (notdiag)
+              atomicAdd(jp + (long long)e * np + cd, v * (D[(long long)a * n + b] + (offab ? D[(long long)b * n + a] : 0.0)));
+          }
+          if (with_k) {
+            double* s = sk + (long long)e * 4 * n;
+            rc[q][0] += v * D[(long long)b * n + d];                          // K[a][c]
+            if (offd) s[d] += v * D[(long long)b * n + c];                    // K[a][d]
+            if (offab) {
+              rc[q][1] += v * D[(long long)a * n + d];                        // K[b][c]
+              if (offd) s[n + d] += v * D[(long long)a * n + c];              // K[b][d]
+            }
+            if (notdiag) {
+              rc[q][2] += v * D[(long long)d * n + b];                        // K[c][a]
+              if (offab) rc[q][3] += v * D[(long long)d * n + a];             // K[c][b]
+              if (offd) {
+                s[2 * n + d] += v * D[(long long)c * n + b];                  // K[d][a]
+                if (offab) s[3 * n + d] += v * D[(long long)c * n + a];       // K[d][b]
+              }
+            }
+          }
         }
       }
-      if (K) {
-        atomicAdd(K + (long long)a * n + c, v * D[(long long)b * n + d]);
-        if (c != d) atomicAdd(K + (long long)a * n + d, v * D[(long long)b * n + c]);
-        if (a != b) atomicAdd(K + (long long)b * n + c, v * D[(long long)a * n + d]);
-        if (a != b && c != d) atomicAdd(K + (long long)b * n + d, v * D[(long long)a * n + c]);
-        if (ab != cd) {
-          atomicAdd(K + (long long)c * n + a, v * D[(long long)d * n + b]);
-          if (a != b) atomicAdd(K + (long long)c * n + b, v * D[(long long)d * n + a]);
-          if (c != d) atomicAdd(K + (long long)d * n + a, v * D[(long long)c * n + b]);
-          if (a != b && c != d) atomicAdd(K + (long long)d * n + b, v * D[(long long)c * n + a]);
-        }
+      if (with_k) {
+        for (int q = 0; q < ne; ++q)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) {
+            double v = rc[q][y];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0) sk[(long long)(e0 + q) * 4 * n + y * n + c] += v;
+          }
       }
+      __syncwarp();
     }
-    if (J) {
-      for (int off = 16; off > 0; off >>= 1) jab += __shfl_down_sync(0xffffffffu, jab, off);
-      if (lane == 0 && jab != 0.0) {
-        atomicAdd(J + (long long)a * n + b, jab);
-        if (a != b) atomicAdd(J + (long long)b * n + a, jab);
+    if (with_j) {
+      for (int q = 0; q < ne; ++q) {
+        double v = jab[q];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0 && v != 0.0) atomicAdd(jp + (long long)(e0 + q) * np + ab, v);
+        jab[q] = 0.0;
       }
     }
   }
+  if (!with_k) return;
+  __syncwarp();
+  // the row's exchange sums: rows a, b and columns a, b of every density's K
+  for (int e = 0; e < nb; ++e) {
+    double* K = out + ((long long)with_j * nb + e) * nn;
+    const double* s = sk + (long long)e * 4 * n;
+    for (int x = lane; x < n; x += 32) {
+      if (s[x] != 0.0) atomicAdd(K + (long long)a * n + x, s[x]);
+      if (s[2 * n + x] != 0.0) atomicAdd(K + (long long)x * n + a, s[2 * n + x]);
+      if (a != b) {
+        if (s[n + x] != 0.0) atomicAdd(K + (long long)b * n + x, s[n + x]);
+        if (s[3 * n + x] != 0.0) atomicAdd(K + (long long)x * n + b, s[3 * n + x]);
+      }
+    }
+  }
+}
+
+// J[i][j] = J[j][i] = jp[pair(i, j)] for every density.
+__global__ void packed_j_out_kernel(const double* __restrict__ jp, int n, long long np, int nb,
+                                    double* __restrict__ out) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nn = (long long)n * n;
+  if (idx >= nn * nb) return;
+  const int e = (int)(idx / nn);
+  const long long r = idx - e * nn;
+  const int i = (int)(r / n), j = (int)(r % n);
+  const long long pr = i >= j ? (long long)i * (i + 1) / 2 + j : (long long)j * (j + 1) / 2 + i;
+  out[idx] = jp[(long long)e * np + pr];
 }
 
 }  // namespace
@@ -90,14 +155,34 @@ extern "C" int b200jk_packed_jk(const double* d_eri, int32_t layout, int64_t eri
     const long long np = (long long)n * (n + 1) / 2;
     if (eri_size != (layout == 1 ? np * (np + 1) / 2 : np * np))
       b200jk::fail_invalid("Packed J/K dimensions do not match");  // csrc/packed_jk.cc:18-22
+    const size_t smem = with_k ? (size_t)4 * n * nb * sizeof(double) : 0;
+    if (smem > 200 * 1024)
+      b200jk::fail_invalid("Packed J/K: n x nb too large for the per-row exchange sums (n * nb <= 6400)");
     cudaStream_t st = (cudaStream_t)stream;
     const size_t outn = (size_t)(with_j + with_k) * nb * n * n;
     cudaError_t e = cudaMemsetAsync(d_out, 0, outn * sizeof(double), st);
     if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
-    const long long warps = np;
-    b200jk::packed_jk_kernel<<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(d_eri, layout, n, np, d_density, nb,
-                                                                        d_out, with_j, with_k);
+    // pair-packed J accumulator (stream-ordered allocation, freed on the stream after use)
+    double* jp = nullptr;
+    if (with_j) {
+      e = cudaMallocAsync(reinterpret_cast<void**>(&jp), (size_t)nb * np * sizeof(double), st);
+      if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+      e = cudaMemsetAsync(jp, 0, (size_t)nb * np * sizeof(double), st);
+      if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+    }
+    static std::atomic<uint64_t> smem_done{0};
+    b200jk::smem_opt_in(b200jk::packed_jk_kernel, smem, smem_done);
+    b200jk::packed_jk_kernel<<<(unsigned)np, 32, smem, st>>>(d_eri, layout, n, np, d_density, nb, d_out, jp,
+                                                            with_j, with_k);
     e = cudaGetLastError();
     if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+    if (with_j) {
+      const long long total = (long long)nb * n * n;
+      b200jk::packed_j_out_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(jp, n, np, nb, d_out);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+      e = cudaFreeAsync(jp, st);
+      if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+    }
   });
 }

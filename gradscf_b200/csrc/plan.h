@@ -119,6 +119,7 @@ struct ProfileEvent {
 #define B200JK_AUX_STREAMS 3
 #endif
 constexpr int kAuxStreams = B200JK_AUX_STREAMS;  // streams besides the caller's for concurrent class-pair launches
+constexpr int kQueueSlots = 4096;  // work-queue counters of persistent launches, reused cyclically
 
 struct Plan {
   int device = 0;
@@ -172,6 +173,9 @@ struct Plan {
   // bumped whenever device work-item arrays are rebuilt or rewritten
   // (autotune, set_shard): a CUDA graph captured before then is stale
   unsigned long long layout_gen = 0;
+  // work-queue counters of the persistent launches: one per unit and slice
+  DevBuf d_queue;            // kQueueSlots ints, allocated with the plan
+  unsigned next_queue = 0;
   double last_fp32_cut = 0.0;   // fp32_cut of the last split-precision build (split statistics)
   // optional per-class launch timing (CUDA events on the launching stream)
   bool profiling = false;
