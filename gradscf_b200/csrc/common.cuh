@@ -365,4 +365,67 @@ __device__ __forceinline__ void build_g(R c00, R c0p, R b10, R b01, R b00, R g00
     }
 }
 
+// The same table with the recursion held in memory instead of registers:
+// the vertical recursion advances one f column at a time (two columns in
+// registers), the ket transfer runs in `w` ((LAB+1)(LCD+1)(LD+1) values,
+// shared or local memory) and the bra transfer per (c, d) keeps one column
+// of LAB+1 values.  For large classes, whose register-held recursion would
+// cap the occupancy of the whole kernel.
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void build_g_mem(R c00, R c0p, R b10, R b01, R b00, R g00, R ab, R cd, R* G,
+                                            R* w) {
+  constexpr int LAB = LA + LB, LCD = LC + LD;
+  auto W = [&](int e, int c, int d) -> R& { return w[(e * (LCD + 1) + c) * (LD + 1) + d]; };
+  R prev[LAB + 1], cur[LAB + 1];
+  cur[0] = g00;
+  if (LAB > 0) cur[1] = c00 * g00;
+#pragma unroll
+  for (int e = 1; e < LAB; ++e) cur[e + 1] = c00 * cur[e] + R(e) * b10 * cur[e - 1];
+#pragma unroll
+  for (int e = 0; e <= LAB; ++e) {
+    W(e, 0, 0) = cur[e];
+    prev[e] = R(0);
+  }
+#pragma unroll
+  for (int f = 0; f < LCD; ++f) {
+    R next[LAB + 1];
+#pragma unroll
+    for (int e = 0; e <= LAB; ++e) {
+      R val = c0p * cur[e];
+      if (f > 0) val += R(f) * b01 * prev[e];
+      if (e > 0) val += R(e) * b00 * cur[e - 1];
+      next[e] = val;
+    }
+#pragma unroll
+    for (int e = 0; e <= LAB; ++e) {
+      prev[e] = cur[e];
+      cur[e] = next[e];
+      W(e, f + 1, 0) = next[e];
+    }
+  }
+#pragma unroll
+  for (int e = 0; e <= LAB; ++e)
+#pragma unroll
+    for (int d = 1; d <= LD; ++d)
+#pragma unroll
+      for (int c = 0; c <= LCD - d; ++c) W(e, c, d) = W(e, c + 1, d - 1) + cd * W(e, c, d - 1);
+#pragma unroll
+  for (int c = 0; c <= LC; ++c)
+#pragma unroll
+    for (int d = 0; d <= LD; ++d) {
+      R y[LAB + 1];
+#pragma unroll
+      for (int e = 0; e <= LAB; ++e) y[e] = W(e, c, d);
+#pragma unroll
+      for (int b = 0; b <= LB; ++b) {
+#pragma unroll
+        for (int a = 0; a <= LA; ++a) G[((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d] = y[a];
+        if (b < LB) {
+#pragma unroll
+          for (int a = 0; a + b < LAB; ++a) y[a] = y[a + 1] + ab * y[a];
+        }
+      }
+    }
+}
+
 }  // namespace b200jk

@@ -125,15 +125,18 @@ inline int persistent_blocks(Kernel* kernel, int threads, size_t smem, std::atom
 // Dynamic shared memory above 48 KB is an opt-in attribute of each kernel in
 // each device's context: set it on the current device the first time a
 // kernel is launched there (bit d of `done` marks device d; any thread).
+// Returns the attribute call's error (cudaSuccess when nothing was needed).
 template <typename Kernel>
-inline void smem_opt_in(Kernel* kernel, size_t bytes, std::atomic<uint64_t>& done) {
-  if (bytes <= 48 * 1024) return;
+inline cudaError_t smem_opt_in(Kernel* kernel, size_t bytes, std::atomic<uint64_t>& done) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return;  // the launch reports the error
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
   const uint64_t bit = dev < 64 ? (uint64_t(1) << dev) : 0;
-  if (bit && (done.load(std::memory_order_acquire) & bit)) return;
-  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess && bit)
-    done.fetch_or(bit, std::memory_order_acq_rel);
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+  return e;
 }
 
 }  // namespace b200jk

@@ -163,6 +163,139 @@ __global__ void grad_team_kernel(JKArgs args) {
 
 namespace b200jk {
 
+// ---------------------------------------------------------------------------
+// Block-wide coordinate VJP for the large classes (NOUT > 256, i.e. d and f
+// shells): the whole block works on one quartet at a time.  Gamma of every
+// element is staged in shared memory once per quartet; per primitive
+// quartet the raised 2D tables of every root and axis are built in shared
+// memory (build_g_mem, one thread per table, recursion scratch in shared
+// memory so the kernel's register count stays that of the accumulation);
+// the threads then stride over the elements, each summing the nine centre
+// partials, which are block-reduced per quartet.
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD>
+struct GradBlk {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using GC = GradCfg<LA, LB, LC, LD, 1>;
+  static constexpr int THREADS = 128;
+  static constexpr int N = GC::NROOT, NG = GC::NG;
+  static constexpr int LAB = LA + LB + 2, LCD = LC + LD + 1;
+  static constexpr int NW = (LAB + 1) * (LCD + 1) * (LD + 1);   // recursion scratch per table
+  static constexpr int G_OFF = 0, R_OFF = 3 * N * NG, W_OFF = R_OFF + 2 * N, GAM_OFF = W_OFF + 3 * N * NW;
+  static constexpr int ELEMS = GAM_OFF + CI::NOUT;
+  static constexpr size_t bytes() { return (size_t)ELEMS * 8; }
+  static constexpr bool OK = CI::NOUT > 256 && bytes() <= 220 * 1024;
+};
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128) grad_block_kernel(JKArgs args) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using GB = GradBlk<LA, LB, LC, LD>;
+  using GC = GradCfg<LA, LB, LC, LD, 1>;
+  constexpr int N = GB::N, NG = GB::NG;
+  extern __shared__ __align__(16) double gsm[];
+  double* G = gsm + GB::G_OFF;
+  double* roots = gsm + GB::R_OFF;
+  double* scratch = gsm + GB::W_OFF;
+  double* gam = gsm + GB::GAM_OFF;
+  __shared__ double red[9][GB::THREADS / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int4 w = args.work[blockIdx.x];
+  const int bra = args.bra_pairs[w.x];
+  for (int k = w.y; k < w.z; ++k) {
+    QuartetGeom g;
+    load_quartet(args, bra, args.ket_pairs[k], g);
+    const long long base = args.mol_base[g.mol];
+    const int n = args.mol_n[g.mol];
+    for (int o = tid; o < CI::NOUT; o += GB::THREADS) {
+      const int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
+      const int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
+      gam[o] = g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id);
+    }
+    double dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
+    for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
+      const double4 P = args.pp_data[i];
+      const double2 PA = args.pp_aux[i];
+      const double alpha = args.pp_exp[i].x, beta = args.pp_exp[i].y;
+      for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
+        PrimQ<double> s;
+        prim_setup<double>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
+        const double gamma_c = args.pp_exp[j].x;
+        __syncthreads();   // the previous primitive quartet's tables are no longer read
+        if (tid < 2 * N) roots[tid] = rys_one<N, double>(s.t, tid, args.tb);
+        __syncthreads();
+        if (tid < 3 * N) {
+          const int r = tid / 3, ax = tid - 3 * r;
+          RootCoef<double> rc;
+          root_coef<double>(s, roots[r], rc);
+          const double abd = ax == 0 ? g.abx : (ax == 1 ? g.aby : g.abz);
+          const double cdd = ax == 0 ? g.cdx : (ax == 1 ? g.cdy : g.cdz);
+          const double g00 = ax == 2 ? roots[N + r] * s.pref : 1.0;
+          build_g_mem<LA + 1, LB + 1, LC + 1, LD, double>(rc.c00[ax], rc.c0p[ax], rc.b10, rc.b01, rc.b00, g00, abd,
+                                                         cdd, G + tid * NG, scratch + tid * GB::NW);
+        }
+        __syncthreads();
+        for (int o = tid; o < CI::NOUT; o += GB::THREADS) {
+          const double gq = gam[o];
+          if (gq == 0.0) continue;
+          const int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
+          const int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
+          const int la[3] = {cart_lx(LA, ia), cart_ly(LA, ia), cart_lz(LA, ia)};
+          const int lb[3] = {cart_lx(LB, ib), cart_ly(LB, ib), cart_lz(LB, ib)};
+          const int lc[3] = {cart_lx(LC, ic), cart_ly(LC, ic), cart_lz(LC, ic)};
+          const int ld[3] = {cart_lx(LD, id), cart_ly(LD, id), cart_lz(LD, id)};
+#pragma unroll 2
+          for (int r = 0; r < N; ++r) {
+            double v[3], fa[3], fb[3], fc[3];
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+              const double* Gx = G + (r * 3 + x) * NG;
+              const int a = la[x], b = lb[x], c = lc[x], d = ld[x];
+              v[x] = Gx[GC::idx(a, b, c, d)];
+              fa[x] = 2.0 * alpha * Gx[GC::idx(a + 1, b, c, d)] - (a ? a * Gx[GC::idx(a - 1, b, c, d)] : 0.0);
+              fb[x] = 2.0 * beta * Gx[GC::idx(a, b + 1, c, d)] - (b ? b * Gx[GC::idx(a, b - 1, c, d)] : 0.0);
+              fc[x] = 2.0 * gamma_c * Gx[GC::idx(a, b, c + 1, d)] - (c ? c * Gx[GC::idx(a, b, c - 1, d)] : 0.0);
+            }
+            const double yz = gq * v[1] * v[2], xz = gq * v[0] * v[2], xy = gq * v[0] * v[1];
+            dA[0] += fa[0] * yz; dA[1] += fa[1] * xz; dA[2] += fa[2] * xy;
+            dB[0] += fb[0] * yz; dB[1] += fb[1] * xz; dB[2] += fb[2] * xy;
+            dC[0] += fc[0] * yz; dC[1] += fc[1] * xz; dC[2] += fc[2] * xy;
+          }
+        }
+      }
+    }
+    // block reduction of the nine partials; thread 0 adds to the four centres
+    double part[9] = {dA[0], dA[1], dA[2], dB[0], dB[1], dB[2], dC[0], dC[1], dC[2]};
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) part[q] += __shfl_down_sync(0xffffffffu, part[q], off);
+      if (lane == 0) red[q][warp] = part[q];
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double sum[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+        sum[q] = 0.0;
+        for (int wi = 0; wi < GB::THREADS / 32; ++wi) sum[q] += red[q][wi];
+      }
+      double* gA = args.grad + 3LL * args.ws_atm[g.A];
+      double* gB = args.grad + 3LL * args.ws_atm[g.B];
+      double* gC = args.grad + 3LL * args.ws_atm[g.C];
+      double* gD = args.grad + 3LL * args.ws_atm[g.D];
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        atomicAdd(gA + x, sum[x]);
+        atomicAdd(gB + x, sum[3 + x]);
+        atomicAdd(gC + x, sum[6 + x]);
+        atomicAdd(gD + x, -(sum[x] + sum[3 + x] + sum[6 + x]));
+      }
+    }
+    __syncthreads();   // red and gam are rewritten by the next quartet
+  }
+}
+
 // Register-path coordinate VJP for small classes: one lane per ket of a
 // work item (warp-granular items as the J/K register path), the raised 2D
 // integrals of one root in registers, nine derivative partials per lane;

@@ -2241,7 +2241,9 @@ int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_
         CUDA_OK(cudaEventRecord(ev.start, ls));
       }
       const int rc = disp.grad64[cls](a, ls);
-      if (rc) throw Failure{B200JK_INTERNAL, std::string("gradient launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
+      if (rc)
+        throw Failure{B200JK_INTERNAL, std::string("gradient launch failed (class pair ") + std::to_string(W->x) + "," +
+                                           std::to_string(W->y) + "): " + cudaGetErrorString((cudaError_t)rc)};
       if (p.profiling) {
         CUDA_OK(cudaEventRecord(ev.stop, ls));
         p.events.push_back(ev);

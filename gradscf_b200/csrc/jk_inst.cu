@@ -141,6 +141,19 @@ int launch_grad(const JKArgs& args, cudaStream_t stream) {
     grad_reg_kernel<LA, LB, LC, LD><<<(args.nwork + 3) / 4, 128, 0, stream>>>(args);
     return (int)cudaGetLastError();
   }
+#ifndef B200JK_GRAD_BLOCK
+#define B200JK_GRAD_BLOCK 1
+#endif
+  if constexpr (B200JK_GRAD_BLOCK && GradBlk<LA, LB, LC, LD>::OK) {
+    // large classes: one quartet per block at a time (block-wide teams)
+    using GB = GradBlk<LA, LB, LC, LD>;
+    constexpr size_t smem = GB::bytes();
+    static std::atomic<uint64_t> smem_done{0};
+    const cudaError_t ea = smem_opt_in(grad_block_kernel<LA, LB, LC, LD>, smem, smem_done);
+    if (ea != cudaSuccess) return (int)ea;
+    grad_block_kernel<LA, LB, LC, LD><<<args.nwork, GB::THREADS, smem, stream>>>(args);
+    return (int)cudaGetLastError();
+  }
   using CI = ClassInfo<LA, LB, LC, LD>;
   constexpr int TEAM = CI::NOUT <= 8 ? 4 : CI::NOUT <= 64 ? 8 : CI::NOUT <= 256 ? 16 : 32;
   using GC = GradCfg<LA, LB, LC, LD, TEAM>;
