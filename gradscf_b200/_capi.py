@@ -23,7 +23,7 @@ EXPORTS = (
     "b200jk_direct_jk_noalloc", "b200jk_graph_create", "b200jk_graph_launch", "b200jk_graph_destroy",
     "b200jk_partition_items", "b200jk_plan_set_shard", "b200jk_plan_autotune",
     "b200jk_packed_eri", "b200jk_packed_jk", "b200jk_plan_launches",
-    "b200jk_direct_jk_geom_jvp", "b200jk_direct_jk_geom_hvp",
+    "b200jk_direct_jk_geom_jvp", "b200jk_direct_jk_geom_hvp", "b200jk_measure_bra_transfer",
 )
 NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024
 NCLASS = 55
@@ -89,6 +89,7 @@ def lib():
     h.b200jk_packed_jk.argtypes = [vp, i32, i64, i32, vp, i32, vp, i32, i32, vp]
     h.b200jk_plan_profile.argtypes = [vp, ctypes.POINTER(f64), ctypes.POINTER(f64), ctypes.POINTER(i32)]
     h.b200jk_measure_fma_peak.argtypes = [i32, ctypes.POINTER(f64), vp]
+    h.b200jk_measure_bra_transfer.argtypes = [i32, i32, ctypes.POINTER(f64), ctypes.POINTER(f64), vp]
     h.b200jk_direct_jk_noalloc.argtypes = [vp, vp, i32, vp, i32, i32, i32, i32, f64, vp]
     h.b200jk_graph_create.argtypes = [vp, vp, i32, vp, i32, i32, i32, i32, f64, ctypes.POINTER(vp)]
     h.b200jk_graph_launch.argtypes = [vp, vp]

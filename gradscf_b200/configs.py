@@ -14,6 +14,8 @@ c4  (H2O)64 cc-pVTZ (3712 functions, seed 4): J/K builds in FP64 and split
     mode along an RHF SCF (fragment guess, 15 iterations) and one force.
 prof  one small run of a kernel family for profiler captures (--case jk |
     grad | packed, --nwater, --basis).
+tcprobe  the f x f bra transfer as the scalar recursion and as an FP64
+    tensor-core GEMM, timed side by side.
 Geometry generator and seeds: gradscf_b200/workloads.py.
 """
 from __future__ import annotations
@@ -93,10 +95,24 @@ def run_c2(nwater=16, seed=2, npick=6):
 
 
 def run_c3(count=256, quick=False):
+    import os
     sizes = W.batch_sizes(count=count, seed=3)
     if quick:
         sizes = sizes[:16]
-    specs = [W.water_cluster(int(nw), 1000 + m) for m, nw in enumerate(sizes)]
+    # several GPUs (torchrun): the clusters run as replicas, a cost-balanced
+    # share per rank, energies gathered on the host at the end
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    mine = np.arange(len(sizes))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        mine = S.replica_shard((24 * np.asarray(sizes, dtype=np.int64)) ** 3, rank, world)
+    all_sizes = sizes
+    sizes = sizes[mine]
+    specs = [W.water_cluster(int(nw), 1000 + int(m)) for m, nw in zip(mine, sizes)]
     batch = S.MoleculeBatch(specs, "cc-pvdz", cart=False, schwarz_cut=1e-12)
     # fragment guess: every monomer of every cluster in one batched SCF
     monomers = [f for spec, nw in zip(specs, sizes) for f in _fragments(spec, int(nw))]
@@ -120,6 +136,24 @@ def run_c3(count=256, quick=False):
                           "quartets_per_s": batch.plan.quartets / (np.mean(steady) * 1e-3)}
     out["split_speedup"] = out["fp64"]["ms_per_build"] / out["split"]["ms_per_build"]
     out["max_abs_dE_per_molecule_hartree"] = float(np.abs(energies["split"] - energies["fp64"]).max())
+    if world > 1:
+        import torch.distributed as dist
+        n = len(all_sizes)
+        e64 = S.gather_replicas(mine, energies["fp64"], n)
+        e32 = S.gather_replicas(mine, energies["split"], n)
+        t = torch.tensor([out["fp64"]["ms_per_build"], out["split"]["ms_per_build"]], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        q = torch.tensor([out["quartets_per_build"]], dtype=torch.float64)
+        dist.all_reduce(q)
+        out = {"config": "c3", "ranks": world, "molecules": n, "scaling": "replicas",
+               "quartets_per_build": int(q.item()),
+               "fp64": {"ms_per_build_max_over_ranks": t[0].item(), "quartets_per_s": q.item() / (t[0].item() * 1e-3)},
+               "split": {"ms_per_build_max_over_ranks": t[1].item(), "quartets_per_s": q.item() / (t[1].item() * 1e-3)},
+               "max_abs_dE_per_molecule_hartree": float(np.nanmax(np.abs(e32 - e64))),
+               "all_molecules_reported": bool(np.all(np.isfinite(e64)))}
+        dist.destroy_process_group()
+        if rank != 0:
+            return None
     return out
 
 
@@ -255,9 +289,24 @@ def run_prof(case="jk", nwater=8, basis="cc-pvdz", seed=1):
     return out
 
 
+def run_tcprobe(ncol=1 << 20, reps=20):
+    """The tensor-core decision for the f x f bra transfer: the scalar
+    recursion against the same linear map as a GEMM on the FP64 tensor cores
+    (b200jk_measure_bra_transfer), ns per (root, axis, ket) column."""
+    import ctypes
+    from . import _capi
+    ns = (ctypes.c_double * 2)()
+    diff = ctypes.c_double()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _capi.check(_capi.lib().b200jk_measure_bra_transfer(ncol, reps, ns, ctypes.byref(diff), st))
+    return {"config": "tcprobe", "transfer": "f x f bra (16 outputs from 7 inputs per column), FP64",
+            "columns": ncol, "reps": reps, "ns_per_column_recursion": ns[0], "ns_per_column_dmma_gemm": ns[1],
+            "max_abs_diff": diff.value}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("config", choices=("c0", "c2", "c3", "c4", "packed", "prof"))
+    ap.add_argument("config", choices=("c0", "c2", "c3", "c4", "packed", "prof", "tcprobe"))
     ap.add_argument("--quick", action="store_true", help="reduced size (smoke run)")
     ap.add_argument("--cycles", type=int, default=15, help="c4: SCF iterations per precision")
     ap.add_argument("--case", default="jk", choices=("jk", "grad", "packed"), help="prof: kernel family")
@@ -266,10 +315,12 @@ def main(argv=None):
     a = ap.parse_args(argv)
     fn = {"c0": run_c0, "c2": run_c2, "c3": lambda: run_c3(quick=a.quick), "packed": run_packed,
           "c4": lambda: run_c4(cycles=a.cycles, quick=a.quick),
-          "prof": lambda: run_prof(a.case, a.nwater, a.basis)}[a.config]
+          "prof": lambda: run_prof(a.case, a.nwater, a.basis), "tcprobe": run_tcprobe}[a.config]
     if a.config == "c2" and a.quick:
         fn = lambda: run_c2(nwater=4)  # noqa: E731
-    print(json.dumps(fn()))
+    res = fn()
+    if res is not None:
+        print(json.dumps(res))
 
 
 if __name__ == "__main__":

@@ -429,6 +429,27 @@ def rhf_batch(batch: MoleculeBatch, *, conv_tol=1e-10, max_cycle=60, precision="
     return energies, densities, times, cycle, converged
 
 
+def replica_shard(costs, rank, world):
+    """The molecules of a batch that rank `rank` of `world` runs when a batch
+    of independent molecules runs as replicas (no collective on the data
+    path): contiguous cost-balanced blocks (b200jk_partition_items).  Returns
+    the molecule indices."""
+    owner = _capi.partition_items(np.asarray(costs, dtype=np.int64), world)
+    return np.nonzero(owner == rank)[0]
+
+
+def gather_replicas(ids, values, count, group=None):
+    """Every rank's per-molecule results (molecule ids -> values) gathered on
+    every rank into one array of `count` (one host all-gather at the end)."""
+    import torch.distributed as dist
+    parts = [None] * dist.get_world_size(group)
+    dist.all_gather_object(parts, ([int(i) for i in ids], [float(v) for v in values]), group=group)
+    out = np.full(count, np.nan)
+    for pid, pval in parts:
+        out[pid] = pval
+    return out
+
+
 def fragment_guess(mol: Molecule, fragments, basis, *, unit="Angstrom"):
     """Block-diagonal guess density from converged RHF densities of the
     fragments (consecutive atoms of `mol`, in order), all solved in one

@@ -129,6 +129,15 @@ int b200jk_packed_jk(const double* d_eri, int32_t layout, int64_t eri_size, int3
  * shard) in `precision` mode. */
 int b200jk_plan_launches(const b200jk_plan* plan, int32_t precision, int64_t* count);
 
+/* Probe for the tensor-core decision on the high-l horizontal transfer (no
+ * counterpart in the reference): times the f x f bra transfer of the 2D
+ * integrals (16 outputs from 7 inputs per root/axis/ket column, FP64) over
+ * `ncol` columns x `reps`, as the scalar recursion (ns_per_column[0]) and as a
+ * GEMM on the FP64 tensor cores (mma.sync DMMA, ns_per_column[1]), and
+ * returns the largest difference between the two results. */
+int b200jk_measure_bra_transfer(int32_t ncol, int32_t reps, double* ns_per_column, double* max_abs_diff,
+                                void* stream);
+
 /* Measured vector-pipe FMA throughput of the current device in TFLOP/s
  * (fp64 = 1: FP64, 0: FP32) -- the roofline denominator for the ERI kernels. */
 int b200jk_measure_fma_peak(int32_t fp64, double* tflops, void* stream);

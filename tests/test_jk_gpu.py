@@ -357,3 +357,15 @@ def test_graph_survives_scratch_growth_and_refuses_stale_work_items():
     out = g.run(torch.as_tensor(d.reshape(1, -1), device="cuda")).cpu().numpy()
     assert np.abs(out[1, 0].reshape(n, n) - k0).max() < 1e-10
     g.close()
+
+
+def test_bra_transfer_probe_variants_agree():
+    # the recursion and the tensor-core GEMM form of the f x f bra transfer
+    # compute the same map (b200jk_measure_bra_transfer)
+    import ctypes
+    ns = (ctypes.c_double * 2)()
+    diff = ctypes.c_double()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _capi.check(_capi.lib().b200jk_measure_bra_transfer(4096, 2, ns, ctypes.byref(diff), st))
+    assert diff.value < 1e-12
+    assert ns[0] > 0 and ns[1] > 0

@@ -121,3 +121,51 @@ def test_two_gloo_ranks_sum_to_full_jk():
     # each rank alone holds only part of the result
     j0, _, _, _ = _partial_jk(0, world)
     assert np.abs(j0 - jref).max() > 1e-3
+
+
+def _replica_worker(rank, world, port, queue):
+    import torch.distributed as dist
+    from gradscf_b200 import scf as S
+    from gradscf_b200 import workloads as Wl
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sizes = Wl.batch_sizes(256, 3)
+        cost = (24 * sizes.astype(np.int64)) ** 3
+        mine = S.replica_shard(cost, rank, world)
+        # stand-in per-molecule results: any function of the molecule id
+        vals = [1.5 * sizes[m] + 1e-3 * m for m in mine]
+        got = S.gather_replicas(mine, vals, len(sizes))
+        queue.put((rank, mine, got, int(cost[mine].sum())))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_batch_replicas_on_two_gloo_ranks():
+    # the 256-cluster batch as replicas: each rank a contiguous cost-balanced
+    # share of the clusters, per-cluster results gathered on every rank
+    world = 2
+    ctx = mp.get_context("spawn")
+    queue = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_replica_worker, args=(r, world, port, queue)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = {}
+    for _ in range(world):
+        r, mine, got, load = queue.get(timeout=240)
+        res[r] = (mine, got, load)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    from gradscf_b200 import workloads as Wl
+    sizes = Wl.batch_sizes(256, 3)
+    want = 1.5 * sizes + 1e-3 * np.arange(256)
+    ids = np.concatenate([res[r][0] for r in range(world)])
+    assert np.array_equal(np.sort(ids), np.arange(256))           # every cluster exactly once
+    for r in range(world):
+        np.testing.assert_allclose(res[r][1], want)                # gathered on every rank
+    loads = [res[r][2] for r in range(world)]
+    cost = (24 * sizes.astype(np.int64)) ** 3
+    assert max(loads) <= cost.sum() / world + cost.max()           # balanced shares
