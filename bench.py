@@ -395,6 +395,7 @@ def main():
                        "abs_dE_hartree": abs(r32.energy - r64.energy),
                        "last_iter_dE_fp64": abs(r64.energies[-1] - r64.energies[-2])},
             "split_fraction_fp32_quartets": float(acc["q32"].sum() / max(1.0, acc["q32"].sum() + acc["q64"].sum())),
+            "split_fraction_fp32_prim_quartets": float(acc["pq32"].sum() / max(1.0, acc["pq32"].sum() + acc["pq64"].sum())),
             "max_abs_dD_timed": [float(x) for x in acc["maxdd"]],
             "e2e": {"value": quartets / (e2e_step * 1e-3), "unit": "quartets/s",
                     "ms_per_step": e2e_step, "h2d_bytes_per_step": int(n * n * 8),

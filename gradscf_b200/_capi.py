@@ -19,6 +19,7 @@ EXPORTS = (
     "b200jk_plan_quartets", "b200jk_plan_block_offsets", "b200jk_direct_jk",
     "b200jk_check_status", "b200jk_direct_jk_tables", "b200jk_direct_jk_geom_vjp",
     "b200jk_int1e", "b200jk_int1e_grad", "b200jk_plan_class_stats", "b200jk_plan_split_stats",
+    "b200jk_plan_border_stats",
     "b200jk_plan_set_profiling", "b200jk_plan_profile", "b200jk_measure_fma_peak",
     "b200jk_direct_jk_noalloc", "b200jk_graph_create", "b200jk_graph_launch", "b200jk_graph_destroy",
     "b200jk_partition_items", "b200jk_plan_set_shard", "b200jk_plan_autotune",
@@ -80,6 +81,7 @@ def lib():
     p64 = ctypes.POINTER(i64)
     h.b200jk_plan_class_stats.argtypes = [vp, p64, p64]
     h.b200jk_plan_split_stats.argtypes = [vp, vp, p64, p64, p64, p64]
+    h.b200jk_plan_border_stats.argtypes = [vp, vp, p64, p64]
     h.b200jk_plan_set_profiling.argtypes = [vp, i32]
     h.b200jk_partition_items.argtypes = [vp, i64, i32, vp]
     h.b200jk_plan_set_shard.argtypes = [vp, i32, i32]

@@ -240,6 +240,10 @@ def run_prof(case="jk", nwater=8, basis="cc-pvdz", seed=1):
     from . import _capi
     lib = _capi.lib()
     nc = _capi.NCLASS
+    q = (ctypes.c_int64 * nc)(); pq = (ctypes.c_int64 * nc)()
+    _capi.check(lib.b200jk_plan_class_stats(plan._h, q, pq))
+    out["class_quartets"] = {"({}{}|{}{})".format(*_capi.QUARTET_CLASSES[c]): [int(q[c]), int(pq[c])]
+                             for c in range(nc) if q[c] > 0}
     for precision in ("fp64", "split"):
         plan.jk_packed(d, hermi=1, precision=precision)   # first use: kernel attributes, module load
         e0, e1 = _events()

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <type_traits>
+#include <utility>
 
 #define B200JK_PI 3.14159265358979323846
 // 2 pi^(5/2): prefactor of the (ss|ss) integral, 2 pi^2.5 / (p q sqrt(p+q)).
@@ -39,6 +40,17 @@ __device__ __forceinline__ void static_for(F&& f) {
     f(std::integral_constant<int, B>{});
     static_for<B + 1, E>(f);
   }
+}
+
+// The same over [0, N) as one fold expression (no recursion depth, so long
+// loops stay inlined).
+template <typename F, int... I>
+__device__ __forceinline__ void static_for_seq(F&& f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void static_for_n(F&& f) {
+  static_for_seq(f, std::make_integer_sequence<int, N>{});
 }
 
 template <int LA, int LB, int LC, int LD>

@@ -33,6 +33,9 @@ struct DispatchTable {
   // the same buckets on the bra-group register path (null: not built)
   JKLauncher grpg64[kQuartetClasses][9] = {};
   JKLauncher grpg32[kQuartetClasses][9] = {};
+  // FP64 flat-list kernels of split builds, per bucket slot (slot 0: plain);
+  // built wherever the bra-group kernels are
+  JKLauncher flat64[kQuartetClasses][9] = {};
   bool grouped[kQuartetClasses] = {};    // the class pair takes grouped lists
   bool reg_path[kQuartetClasses] = {};   // either precision runs the register path
   bool tile[kQuartetClasses] = {};       // the FP64 kernel is the tile path

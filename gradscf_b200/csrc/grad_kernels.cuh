@@ -418,4 +418,328 @@ __global__ void __launch_bounds__(128, 3) grad_reg_kernel(JKArgs args) {
   }
 }
 
+// Warp-per-quartet coordinate VJP for the classes between the lane kernel
+// and the block kernel (up to 48 KB of tables per warp).  Per primitive
+// quartet the raised 2D tables of every (root, axis) are built in shared
+// memory (build_g_mem, recursion scratch in shared memory, so the kernel's
+// registers stay those of the accumulation), then turned into derivative
+// tables: for every unraised (a, b, c, d) tuple the four values
+// (G, 2 alpha G(a+1) - a G(a-1), 2 beta G(b+1) - b G(b-1),
+// 2 gamma G(c+1) - c G(c-1)) side by side, so an element's nine partials at
+// one root take six 16-byte shared loads.  Lanes stride over the elements;
+// Gamma is staged in shared memory once per quartet.
+template <int LA, int LB, int LC, int LD>
+struct GradWarp {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using GC = GradCfg<LA, LB, LC, LD, 1>;
+  static constexpr int N = GC::NROOT, NGR = GC::NG;
+  static constexpr int NGU = CI::NG;                                     // unraised tuples
+  static constexpr int NW = (LA + LB + 3) * (LC + LD + 2) * (LD + 1);   // build_g_mem scratch
+  static constexpr int D_OFF = (3 * N * NGR + 1) / 2 * 2;                // 16-byte aligned
+  // the derivative tables overwrite the recursion scratch (dead by then)
+  static constexpr int DW = 3 * N * NGU * 4 > 3 * N * NW ? 3 * N * NGU * 4 : 3 * N * NW;
+  static constexpr int GAM_OFF = D_OFF + DW;
+  static constexpr int R_OFF = GAM_OFF + CI::NOUT;
+  static constexpr int ELEMS = (R_OFF + 2 * N + 1) / 2 * 2;
+  static constexpr int WARPS = 4;
+  static constexpr int NK = (CI::NOUT + 31) / 32;
+  static constexpr size_t bytes() { return (size_t)WARPS * ELEMS * sizeof(double); }
+  // the classes where it beat the team / block kernel, measured per class
+  // on (H2O)16 cc-pVTZ (one VJP, serial launches): (21|21) 1.39x, (31|30)
+  // 1.61x, (33|10) 1.42x, (30|30) 1.38x, (33|00) 1.30x, (31|20) 1.25x,
+  // (31|11) 1.22x, (33|20) 1.20x, (32|10) 1.18x, (22|20) 1.12x, (32|30)
+  // 1.08x, (22|11) 1.05x, (30|22) 1.04x, (31|21) 1.03x, (22|21) 1.02x;
+  // elsewhere it was slower (to 0.69x) and is not used
+  static constexpr bool PICK = (LA == 2 && LB == 1 && LC == 2 && LD == 1) || (LA == 3 && LB == 1 && LC == 3 && LD == 0) ||
+                               (LA == 3 && LB == 3 && LC == 1 && LD == 0) || (LA == 3 && LB == 0 && LC == 3 && LD == 0) ||
+                               (LA == 3 && LB == 3 && LC == 0 && LD == 0) || (LA == 3 && LB == 1 && LC == 2 && LD == 0) ||
+                               (LA == 3 && LB == 1 && LC == 1 && LD == 1) || (LA == 3 && LB == 3 && LC == 2 && LD == 0) ||
+                               (LA == 3 && LB == 2 && LC == 1 && LD == 0) || (LA == 2 && LB == 2 && LC == 2 && LD == 0) ||
+                               (LA == 3 && LB == 2 && LC == 3 && LD == 0) || (LA == 2 && LB == 2 && LC == 1 && LD == 1) ||
+                               (LA == 3 && LB == 0 && LC == 2 && LD == 2) || (LA == 3 && LB == 1 && LC == 2 && LD == 1) ||
+                               (LA == 2 && LB == 2 && LC == 2 && LD == 1);
+  static constexpr bool OK = PICK && NGU <= 256 && ELEMS * sizeof(double) <= 48 * 1024;
+};
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128) grad_warp_kernel(JKArgs args) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using GW = GradWarp<LA, LB, LC, LD>;
+  using GC = GradCfg<LA, LB, LC, LD, 1>;
+  constexpr int N = GW::N, NGR = GW::NGR, NGU = GW::NGU;
+  extern __shared__ __align__(16) double wsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* G = wsm + warp * GW::ELEMS;
+  double* D = G + GW::D_OFF;
+  double* scratch = D;
+  double* gam = G + GW::GAM_OFF;
+  double* roots = G + GW::R_OFF;
+  // the lane's elements: unraised tuple index per axis, 8 bits each
+  int tix[GW::NK];
+#pragma unroll
+  for (int q = 0; q < GW::NK; ++q) {
+    const int o = lane + 32 * q;
+    tix[q] = 0;
+    if (o < CI::NOUT) {
+      const int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
+      const int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
+      const int tx = GIdx<LA, LB, LC, LD>::idx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
+      const int ty = GIdx<LA, LB, LC, LD>::idx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
+      const int tz = GIdx<LA, LB, LC, LD>::idx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
+      tix[q] = tx | (ty << 8) | (tz << 16);
+    }
+  }
+  const int4 w = args.work[blockIdx.x];
+  const int bra = args.bra_pairs[w.x];
+  for (int k = w.y + warp; k < w.z; k += GW::WARPS) {
+    QuartetGeom g;
+    load_quartet(args, bra, args.ket_pairs[k], g);
+    const long long base = args.mol_base[g.mol];
+    const int n = args.mol_n[g.mol];
+    for (int o = lane; o < CI::NOUT; o += 32) {
+      const int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
+      const int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
+      gam[o] = g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id);
+    }
+    double dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
+    for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
+      const double4 P = args.pp_data[i];
+      const double2 PA = args.pp_aux[i];
+      const double alpha = args.pp_exp[i].x, beta = args.pp_exp[i].y;
+      for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
+        PrimQ<double> s;
+        prim_setup<double>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
+        const double gamma_c = args.pp_exp[j].x;
+        __syncwarp();   // the previous primitive quartet's tables are no longer read
+        if (lane < 2 * N) roots[lane] = rys_one<N, double>(s.t, lane, args.tb);
+        __syncwarp();
+        if (lane < 3 * N) {
+          const int r = lane / 3, ax = lane - 3 * r;
+          RootCoef<double> rc;
+          root_coef<double>(s, roots[r], rc);
+          const double abd = ax == 0 ? g.abx : (ax == 1 ? g.aby : g.abz);
+          const double cdd = ax == 0 ? g.cdx : (ax == 1 ? g.cdy : g.cdz);
+          const double g00 = ax == 2 ? roots[N + r] * s.pref : 1.0;
+          build_g_mem<LA + 1, LB + 1, LC + 1, LD, double>(rc.c00[ax], rc.c0p[ax], rc.b10, rc.b01, rc.b00, g00, abd,
+                                                         cdd, G + lane * NGR, scratch + lane * GW::NW);
+        }
+        __syncwarp();
+        const double e2a = 2.0 * alpha, e2b = 2.0 * beta, e2c = 2.0 * gamma_c;
+        for (int e = lane; e < 3 * N * NGU; e += 32) {
+          const int tbl = e / NGU, tt = e - tbl * NGU;
+          const int d = tt % (LD + 1), c = (tt / (LD + 1)) % (LC + 1);
+          const int b = (tt / ((LD + 1) * (LC + 1))) % (LB + 1), a = tt / ((LD + 1) * (LC + 1) * (LB + 1));
+          const double* Gt = G + tbl * NGR;
+          const double v = Gt[GC::idx(a, b, c, d)];
+          double fa = e2a * Gt[GC::idx(a + 1, b, c, d)];
+          double fb = e2b * Gt[GC::idx(a, b + 1, c, d)];
+          double fc = e2c * Gt[GC::idx(a, b, c + 1, d)];
+          if (a) fa -= a * Gt[GC::idx(a - 1, b, c, d)];
+          if (b) fb -= b * Gt[GC::idx(a, b - 1, c, d)];
+          if (c) fc -= c * Gt[GC::idx(a, b, c - 1, d)];
+          double2* De = reinterpret_cast<double2*>(D + 4 * e);
+          De[0] = make_double2(v, fa);
+          De[1] = make_double2(fb, fc);
+        }
+        __syncwarp();
+        const double2* D2 = reinterpret_cast<const double2*>(D);
+#pragma unroll
+        for (int q = 0; q < GW::NK; ++q) {
+          const int o = lane + 32 * q;
+          if (o >= CI::NOUT) break;
+          const double gq = gam[o];
+          if (gq == 0.0) continue;
+          const int tx = tix[q] & 255, ty = (tix[q] >> 8) & 255, tz = tix[q] >> 16;
+#pragma unroll 2
+          for (int r = 0; r < N; ++r) {
+            const double2* Dr = D2 + 2 * (3 * r * NGU);
+            const double2 x0 = Dr[2 * tx], x1 = Dr[2 * tx + 1];
+            const double2 y0 = Dr[2 * (NGU + ty)], y1 = Dr[2 * (NGU + ty) + 1];
+            const double2 z0 = Dr[2 * (2 * NGU + tz)], z1 = Dr[2 * (2 * NGU + tz) + 1];
+            const double yz = gq * y0.x * z0.x, xz = gq * x0.x * z0.x, xy = gq * x0.x * y0.x;
+            dA[0] += x0.y * yz; dA[1] += y0.y * xz; dA[2] += z0.y * xy;
+            dB[0] += x1.x * yz; dB[1] += y1.x * xz; dB[2] += z1.x * xy;
+            dC[0] += x1.y * yz; dC[1] += y1.y * xz; dC[2] += z1.y * xy;
+          }
+        }
+      }
+    }
+    // warp reduction of the nine partials; lane 0 adds to the four centres
+    double part[9] = {dA[0], dA[1], dA[2], dB[0], dB[1], dB[2], dC[0], dC[1], dC[2]};
+#pragma unroll
+    for (int x = 0; x < 9; ++x)
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) part[x] += __shfl_down_sync(0xffffffffu, part[x], off);
+    if (lane == 0) {
+      double* gA = args.grad + 3LL * args.ws_atm[g.A];
+      double* gB = args.grad + 3LL * args.ws_atm[g.B];
+      double* gC = args.grad + 3LL * args.ws_atm[g.C];
+      double* gD = args.grad + 3LL * args.ws_atm[g.D];
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        atomicAdd(gA + x, part[x]);
+        atomicAdd(gB + x, part[3 + x]);
+        atomicAdd(gC + x, part[6 + x]);
+        atomicAdd(gD + x, -(part[x] + part[3 + x] + part[6 + x]));
+      }
+    }
+    __syncwarp();   // Gamma is rewritten by the next quartet
+  }
+}
+
+// Per-lane coordinate VJP for the mid-size classes (NOUT <= 90): one lane
+// per ket of a work item as the register path, Gamma of the lane's quartet
+// in a private column of shared memory (conflict-free: element-major,
+// lane-minor), and per root the derivative tables of one centre at a time
+// in registers -- raised in a for d/dA, in b for d/dB, in c for d/dC (three
+// smaller tables instead of one raised in all three, so a table set fits
+// the registers).  Every index is a compile-time constant.
+template <int LA, int LB, int LC, int LD>
+struct GradLane {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  static constexpr int NGA = (LA + 2) * (LB + 1) * (LC + 1) * (LD + 1);
+  static constexpr int NGB = (LA + 1) * (LB + 2) * (LC + 1) * (LD + 1);
+  static constexpr int NGC = (LA + 1) * (LB + 1) * (LC + 2) * (LD + 1);
+  static constexpr int NGMAX = NGA > NGB ? (NGA > NGC ? NGA : NGC) : (NGB > NGC ? NGB : NGC);
+  static constexpr int THREADS = 128;
+  static constexpr size_t bytes() { return (size_t)CI::NOUT * THREADS * sizeof(double); }
+#ifndef B200JK_GRAD_LANE_TABLES
+#define B200JK_GRAD_LANE_TABLES 90   // doubles of one centre's three tables
+#endif
+  // measured on (H2O)16 cc-pVTZ: 1.5-2.6x over the team kernel up to 90
+  // elements, slower than the register kernel on its classes and than the
+  // team kernel on 108-element blocks
+  static constexpr bool OK = !GradReg<LA, LB, LC, LD>::OK && CI::NOUT <= 90 && 3 * NGMAX <= B200JK_GRAD_LANE_TABLES;
+};
+
+// One shared-memory load the compiler keeps in place: each centre pass
+// re-reads Gamma instead of holding NOUT values live across the passes.
+__device__ __forceinline__ double lds_keep(const double* p) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"((unsigned)__cvta_generic_to_shared(p)));
+  return v;
+}
+
+// d/dX of one centre (X = 0: A, 1: B, 2: C) for every element of the lane's
+// quartet at one root: tables raised in X's index, Gamma from the lane's
+// shared-memory column, partials into d[3].
+template <int LA, int LB, int LC, int LD, int X>
+__device__ __forceinline__ void grad_lane_centre(const RootCoef<double>& rc, double g00, const QuartetGeom& g,
+                                                 double expo, const double* __restrict__ gam, double* d) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  constexpr int RA = LA + (X == 0), RB = LB + (X == 1), RC = LC + (X == 2);
+  using GI = GIdx<RA, RB, RC, LD>;
+  constexpr int NGX = (RA + 1) * (RB + 1) * (RC + 1) * (LD + 1);
+  double G[3][NGX];
+  build_g<RA, RB, RC, LD, double>(rc.c00[0], rc.c0p[0], rc.b10, rc.b01, rc.b00, 1.0, g.abx, g.cdx, G[0]);
+  build_g<RA, RB, RC, LD, double>(rc.c00[1], rc.c0p[1], rc.b10, rc.b01, rc.b00, 1.0, g.aby, g.cdy, G[1]);
+  build_g<RA, RB, RC, LD, double>(rc.c00[2], rc.c0p[2], rc.b10, rc.b01, rc.b00, g00, g.abz, g.cdz, G[2]);
+  const double e2 = 2.0 * expo;
+  // compile-time element indices: the tables stay in registers
+  static_for_n<CI::NOUT>([&](auto O) {
+    constexpr int o = decltype(O)::value;
+    constexpr int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
+    constexpr int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
+    double v[3], f[3];
+    static_for_n<3>([&](auto AX) {
+      constexpr int ax = decltype(AX)::value;
+      constexpr int a = ax == 0 ? cart_lx(LA, ia) : ax == 1 ? cart_ly(LA, ia) : cart_lz(LA, ia);
+      constexpr int b = ax == 0 ? cart_lx(LB, ib) : ax == 1 ? cart_ly(LB, ib) : cart_lz(LB, ib);
+      constexpr int c = ax == 0 ? cart_lx(LC, ic) : ax == 1 ? cart_ly(LC, ic) : cart_lz(LC, ic);
+      constexpr int dd = ax == 0 ? cart_lx(LD, id) : ax == 1 ? cart_ly(LD, id) : cart_lz(LD, id);
+      constexpr int n = X == 0 ? a : X == 1 ? b : c;   // the raised index
+      v[ax] = G[ax][GI::idx(a, b, c, dd)];
+      f[ax] = e2 * G[ax][GI::idx(a + (X == 0), b + (X == 1), c + (X == 2), dd)];
+      if constexpr (n > 0) f[ax] -= n * G[ax][GI::idx(a - (X == 0), b - (X == 1), c - (X == 2), dd)];
+    });
+    const double gq = lds_keep(gam + o * GradLane<LA, LB, LC, LD>::THREADS);
+    d[0] += gq * f[0] * (v[1] * v[2]);
+    d[1] += gq * f[1] * (v[0] * v[2]);
+    d[2] += gq * f[2] * (v[0] * v[1]);
+  });
+}
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128) grad_lane_kernel(JKArgs args) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  using GC = GradCfg<LA, LB, LC, LD, 1>;
+  using GL = GradLane<LA, LB, LC, LD>;
+  constexpr int N = GC::NROOT;
+  extern __shared__ double s_gam[];   // [NOUT][THREADS]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.x * (GL::THREADS / 32) + warp;
+  if (item >= args.nwork) return;
+  double* gam = s_gam + threadIdx.x;
+  const int4 w = args.work[item];
+  const int bra = args.bra_pairs[w.x];
+  double bA[3] = {0, 0, 0}, bB[3] = {0, 0, 0};
+  int atA = 0, atB = 0;
+  for (int k0 = w.y; k0 < w.z; k0 += 32) {
+    const bool active = k0 + lane < w.z;
+    const int k = active ? k0 + lane : w.z - 1;
+    QuartetGeom g;
+    load_quartet(args, bra, args.ket_pairs[k], g);
+    atA = args.ws_atm[g.A];
+    atB = args.ws_atm[g.B];
+    const long long base = args.mol_base[g.mol];
+    const int n = args.mol_n[g.mol];
+    for (int o = 0; o < CI::NOUT; ++o) {
+      const int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
+      const int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
+      gam[o * GL::THREADS] =
+          active ? g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id) : 0.0;
+    }
+    double dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
+    for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
+      const double4 P = args.pp_data[i];
+      const double2 PA = args.pp_aux[i];
+      const double alpha = args.pp_exp[i].x, beta = args.pp_exp[i].y;
+      for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
+        PrimQ<double> s;
+        prim_setup<double>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
+        const double gamma_c = args.pp_exp[j].x;
+        double x[N], wt[N];
+        rys_roots<N, double>(s.t, x, wt, args.tb);
+        // one (root, centre) pass per iteration, not unrolled: one centre's
+        // tables are live at a time
+#pragma unroll 1
+        for (int tsk = 0; tsk < 3 * N; ++tsk) {
+          const int r = tsk / 3, cx = tsk - 3 * r;
+          RootCoef<double> rc;
+          root_coef<double>(s, x[r], rc);
+          const double g00 = wt[r] * s.pref;
+          if (cx == 0) grad_lane_centre<LA, LB, LC, LD, 0>(rc, g00, g, alpha, gam, dA);
+          else if (cx == 1) grad_lane_centre<LA, LB, LC, LD, 1>(rc, g00, g, beta, gam, dB);
+          else grad_lane_centre<LA, LB, LC, LD, 2>(rc, g00, g, gamma_c, gam, dC);
+        }
+      }
+    }
+    if (active) {
+      double* gC = args.grad + 3LL * args.ws_atm[g.C];
+      double* gD = args.grad + 3LL * args.ws_atm[g.D];
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        atomicAdd(gC + x, dC[x]);
+        atomicAdd(gD + x, -(dA[x] + dB[x] + dC[x]));
+        bA[x] += dA[x];
+        bB[x] += dB[x];
+      }
+    }
+  }
+#pragma unroll
+  for (int x = 0; x < 3; ++x)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      bA[x] += __shfl_down_sync(0xffffffffu, bA[x], off);
+      bB[x] += __shfl_down_sync(0xffffffffu, bB[x], off);
+    }
+  if (lane == 0) {
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      atomicAdd(args.grad + 3LL * atA + x, bA[x]);
+      atomicAdd(args.grad + 3LL * atB + x, bB[x]);
+    }
+  }
+}
+
 }  // namespace b200jk

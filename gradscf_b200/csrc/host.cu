@@ -465,6 +465,65 @@ __global__ void grp_split_kernel(const int4* __restrict__ work, int nwork, const
   if (lane == 0) m_out[i] = dmax;
 }
 
+// Split builds, per bra-group item (one warp): its FP64 quartets (Q_bra
+// Q_ket >= cut, canonical, not Q_bra Q_ket M_item < fp32_cut -- the
+// bra-group kernels' own tests) are appended to the flat list and the item
+// is flagged so the bra-group FP64 launch skips it (the FP64 quartets of an
+// item are the leading kets of its leading bras: on the bra-group path most
+// lanes of their passes idle).  A reservation past the list's capacity is
+// filled with (-1, -1) and its item stays on the bra-group path.  Kets of an
+// item are sorted by bound (descending), so a bra's scan stops at the first
+// pass that starts in FP32.
+__global__ void border_kernel(const int4* __restrict__ work, int nwork, const int* __restrict__ bord,
+                              const double* __restrict__ bra_q, const double* __restrict__ ket_q,
+                              const double* __restrict__ item_m, int same_list, double cut, double fp32_cut,
+                              int2* __restrict__ flat, unsigned long long* __restrict__ flat_n, int cap,
+                              int* __restrict__ skip) {
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= nwork) return;
+  const int4 w = work[i];
+  const double qm = item_m[i];
+  auto scan = [&](auto&& visit) {
+    for (int bi = 0; bi < w.y; ++bi) {
+      const int pos = bord[w.x + bi];
+      const double qb = bra_q[pos];
+      for (int k0 = w.z; k0 < w.w; k0 += 32) {
+        const double q0 = qb * ket_q[k0];
+        if (q0 < cut || q0 * qm < fp32_cut) break;   // this pass and the later ones hold no FP64 quartet
+        const int k = k0 + lane;
+        bool act = false;
+        if (k < w.w) {
+          const double qq = qb * ket_q[k];
+          act = qq >= cut && (!same_list || k <= pos) && !(qq * qm < fp32_cut);
+        }
+        visit(pos, k, act, __ballot_sync(0xffffffffu, act));
+      }
+    }
+  };
+  int count = 0;
+  scan([&](int, int, bool, unsigned b) { count += __popc(b); });
+  if (count == 0) {
+    if (lane == 0) skip[i] = 1;
+    return;
+  }
+  // 64-bit reservation counter: the counts of one build can pass 2^31
+  long long base = 0;
+  if (lane == 0) base = (long long)atomicAdd(flat_n, (unsigned long long)count);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (base + count > (long long)cap) {
+    for (long long j = base + lane; j < (long long)cap && j < base + count; j += 32) flat[j] = make_int2(-1, -1);
+    if (lane == 0) skip[i] = 0;
+    return;
+  }
+  int at = (int)base;
+  scan([&](int pos, int k, bool act, unsigned b) {
+    if (act) flat[at + __popc(b & ((1u << lane) - 1u))] = make_int2(pos, k);
+    at += __popc(b);
+  });
+  if (lane == 0) skip[i] = 1;
+}
+
 // ---------------------------------------------------------------- plan creation
 static int ncart_of(int l) { return (l + 1) * (l + 2) / 2; }
 static int pc_la_host(int pc) { return pc == 0 ? 0 : pc <= 2 ? 1 : pc <= 5 ? 2 : 3; }
@@ -759,6 +818,13 @@ static void fill_group(GroupWork& G, const ClassList& X, const ClassList& Y, boo
   if (!G.all_items.empty())
     CUDA_OK(cudaMemcpy(G.work.ptr, G.all_items.data(), G.all_items.size() * sizeof(int4), cudaMemcpyHostToDevice));
   CUDA_OK(G.m.ensure(std::max<size_t>(G.all_items.size(), 1) * sizeof(double)));
+  // the FP64 flat list of split builds: room for 1/16 of the group's (bra,
+  // ket) pairs, at most 2^21; items that do not fit keep the bra-group path
+  const long long pairs = G.quartets / std::max(1, gb * gk);
+  G.flat_cap = (int)std::min<long long>(pairs / 16 + 4096, 1LL << 21);
+  CUDA_OK(G.flat.ensure((size_t)G.flat_cap * sizeof(int2)));
+  CUDA_OK(G.flat_n.ensure(sizeof(unsigned long long)));
+  CUDA_OK(G.skip.ensure(std::max<size_t>(G.all_items.size(), 1) * sizeof(int)));
 }
 
 // (Re)build the work items of class pair W: the expanded items and, where
@@ -1487,6 +1553,14 @@ static void split_units(Plan& p, ClassPairWork& W, double fp32_cut, cudaStream_t
           u.Y->d_kmax.as<double>(), p.d_rowmax.as<double>(), p.d_mol_ao_off.as<int>(), ncart_of(la),
           ncart_of(lb), u.split->as<double>());
       CUDA_OK(cudaGetLastError());
+      if (u.grp->flat_cap > 0 && dispatch().flat64[quartet_class(W.x, W.y)][gen_slot(u.gb, u.gk)]) {
+        CUDA_OK(cudaMemsetAsync(u.grp->flat_n.ptr, 0, sizeof(unsigned long long), st));
+        border_kernel<<<(u.nwork + 3) / 4, 128, 0, st>>>(
+            u.work->as<int4>(), u.nwork, u.X->d_bord.as<int>(), u.X->d_q.as<double>(), u.Y->d_q.as<double>(),
+            u.split->as<double>(), W.x == W.y, p.cutoff, fp32_cut, u.grp->flat.as<int2>(),
+            u.grp->flat_n.as<unsigned long long>(), u.grp->flat_cap, u.grp->skip.as<int>());
+        CUDA_OK(cudaGetLastError());
+      }
       return;
     }
     SplitLists L{u.X->d_ix.as<int4>(), u.X->d_gx.as<int4>(), u.X->d_gy.as<int4>(), u.Y->d_kmax.as<double>(),
@@ -1521,8 +1595,16 @@ static void launch_units(Plan& p, ClassPairWork& W, JKArgs a, int precision, cud
     const JKLauncher l32 = u.grp ? (plain ? disp.grp32[cls] : disp.grpg32[cls][gs])
                                  : (plain ? disp.jk32[cls] : disp.jkg32[cls][gs]);
     if (!l64 || !l32) throw Failure{B200JK_INTERNAL, "no kernel for this contraction grouping"};
+    const JKLauncher lflat = u.grp ? disp.flat64[cls][gs] : nullptr;
     auto launch = [&](int mode, bool fp32) {
       a.split_mode = mode;
+      // the FP64 slice of a split build: the flat list first, then the
+      // bra-group items it does not hold
+      const bool flat = mode == 1 && lflat && u.grp->flat_cap > 0;
+      a.flat = flat ? u.grp->flat.as<int2>() : nullptr;
+      a.flat_n = flat ? u.grp->flat_n.as<unsigned long long>() : nullptr;
+      a.flat_cap = flat ? u.grp->flat_cap : 0;
+      a.item_skip = flat ? u.grp->skip.as<int>() : nullptr;
       if (u.grp) {
         // a zeroed work-queue counter of its own (slots cycle over the plan's pool)
         int* q = p.d_queue.as<int>() + (p.next_queue++ % kQueueSlots);
@@ -1535,7 +1617,8 @@ static void launch_units(Plan& p, ClassPairWork& W, JKArgs a, int precision, cud
         CUDA_OK(cudaEventCreate(&ev.stop));
         CUDA_OK(cudaEventRecord(ev.start, st));
       }
-      const int rc = fp32 ? l32(a, st) : l64(a, st);
+      int rc = flat ? lflat(a, st) : 0;
+      if (rc == 0) rc = fp32 ? l32(a, st) : l64(a, st);
       if (rc) throw Failure{B200JK_INTERNAL, std::string("J/K launch failed: ") + cudaGetErrorString((cudaError_t)rc)};
       if (p.profiling && allow_profiling) {
         CUDA_OK(cudaEventRecord(ev.stop, st));
@@ -1978,13 +2061,19 @@ int b200jk_plan_launches(const b200jk_plan* plan, int32_t precision, int64_t* co
   return guarded([&] {
     if (!plan || !count) invalid("Invalid plan query");
     const Plan& p = *plan->p;
-    long long units = 0, lists = 0;
+    long long units = 0, lists = 0, flat = 0;
+    const auto& disp = dispatch();
     for (auto* W : p.work)
-      for_each_unit(const_cast<Plan&>(p), *W, [&](const JKUnit& u) { units += u.nwork > 0; });
+      for_each_unit(const_cast<Plan&>(p), *W, [&](const JKUnit& u) {
+        units += u.nwork > 0;
+        flat += u.nwork > 0 && u.grp && u.grp->flat_cap > 0 &&
+                disp.flat64[quartet_class(W->x, W->y)][gen_slot(u.gb, u.gk)] != nullptr;
+      });
     for (int c = 0; c < kPairClasses; ++c) lists += !p.classes[c].q.empty() + !p.grouped[c].q.empty();
     // density_in + jk_out; split: to_float, maxabs, rowmax, one row-max pass
-    // per list, one boundary kernel and two J/K slices per unit
-    *count = precision == B200JK_SPLIT ? 2 + 3 + lists + 3 * units : 2 + units;
+    // per list, one boundary kernel and two J/K slices per unit, and per
+    // bra-group unit the flat-list builder and the flat FP64 kernel
+    *count = precision == B200JK_SPLIT ? 2 + 3 + lists + 3 * units + 2 * flat : 2 + units;
   });
 }
 
@@ -2081,6 +2170,25 @@ int b200jk_plan_split_stats(b200jk_plan* plan, void* stream, int64_t* q64, int64
         }
       });
     }
+  });
+}
+
+int b200jk_plan_border_stats(b200jk_plan* plan, void* stream, int64_t* listed, int64_t* overflow) {
+  return guarded([&] {
+    if (!plan || !listed || !overflow) invalid("Invalid plan query");
+    Plan& p = *plan->p;
+    CUDA_OK(cudaSetDevice(p.device));
+    CUDA_OK(cudaStreamSynchronize((cudaStream_t)stream));
+    *listed = *overflow = 0;
+    for (auto* W : p.work)
+      for_each_unit(p, *W, [&](const JKUnit& u) {
+        if (u.nwork == 0 || !u.grp || u.grp->flat_cap <= 0) return;
+        unsigned long long n = 0;
+        CUDA_OK(cudaMemcpy(&n, u.grp->flat_n.ptr, sizeof(n), cudaMemcpyDeviceToHost));
+        const long long cap = u.grp->flat_cap;
+        *listed += std::min((long long)n, cap);
+        *overflow += std::max(0LL, (long long)n - cap);
+      });
   });
 }
 

@@ -108,6 +108,18 @@ int launch_grp_gen(const JKArgs& args, cudaStream_t stream) {
   return (int)cudaGetLastError();
 }
 
+// The FP64 flat list of a split build: its length is on the device, so the
+// grid is one wave of resident blocks, sized for the list's capacity.
+template <int LA, int LB, int LC, int LD, int GB, int GK>
+int launch_flat(const JKArgs& args, cudaStream_t stream) {
+  if (args.flat_cap <= 0) return 0;
+  static std::atomic<int> resident[64];
+  const int wave = persistent_blocks(jk_flat_kernel<LA, LB, LC, LD, GB, GK>, 128, 0, resident);
+  const int blocks = std::min((args.flat_cap + 127) / 128, wave);
+  jk_flat_kernel<LA, LB, LC, LD, GB, GK><<<blocks, 128, 0, stream>>>(args);
+  return (int)cudaGetLastError();
+}
+
 template <int LA, int LB, int LC, int LD, typename R, int GB, int GK>
 int launch_gen(const JKArgs& args, cudaStream_t stream) {
   if (args.nwork <= 0) return 0;
@@ -137,8 +149,35 @@ int launch_schwarz(const JKArgs& args, int npairs, int cart, cudaStream_t stream
 template <int LA, int LB, int LC, int LD>
 int launch_grad(const JKArgs& args, cudaStream_t stream) {
   if (args.nwork <= 0) return 0;
+#ifndef B200JK_GRAD_LANE
+#define B200JK_GRAD_LANE 1
+#endif
+  if constexpr (B200JK_GRAD_LANE && GradLane<LA, LB, LC, LD>::OK) {
+    // mid-size classes: one lane per quartet, Gamma in shared memory
+    using GL = GradLane<LA, LB, LC, LD>;
+    constexpr size_t smem = GL::bytes();
+    static std::atomic<uint64_t> smem_done{0};
+    const cudaError_t ea = smem_opt_in(grad_lane_kernel<LA, LB, LC, LD>, smem, smem_done);
+    if (ea != cudaSuccess) return (int)ea;
+    grad_lane_kernel<LA, LB, LC, LD><<<(args.nwork + GL::THREADS / 32 - 1) / (GL::THREADS / 32), GL::THREADS,
+                                       smem, stream>>>(args);
+    return (int)cudaGetLastError();
+  }
   if constexpr (GradReg<LA, LB, LC, LD>::OK) {
     grad_reg_kernel<LA, LB, LC, LD><<<(args.nwork + 3) / 4, 128, 0, stream>>>(args);
+    return (int)cudaGetLastError();
+  }
+#ifndef B200JK_GRAD_WARP
+#define B200JK_GRAD_WARP 1
+#endif
+  if constexpr (B200JK_GRAD_WARP && GradWarp<LA, LB, LC, LD>::OK) {
+    // the classes between: one warp per quartet, derivative tables in shared memory
+    using GW = GradWarp<LA, LB, LC, LD>;
+    constexpr size_t smem = GW::bytes();
+    static std::atomic<uint64_t> smem_done{0};
+    const cudaError_t ea = smem_opt_in(grad_warp_kernel<LA, LB, LC, LD>, smem, smem_done);
+    if (ea != cudaSuccess) return (int)ea;
+    grad_warp_kernel<LA, LB, LC, LD><<<args.nwork, 32 * GW::WARPS, smem, stream>>>(args);
     return (int)cudaGetLastError();
   }
 #ifndef B200JK_GRAD_BLOCK
@@ -204,6 +243,7 @@ void register_gen(DispatchTable& t, int id) {
     if constexpr (GRP_GEN && GrpGenAcc<XA, XB, YA, YB, GB, GK>::N <= 26) {
       t.grpg64[id][3 * gslot(GB) + gslot(GK)] = &launch_grp_gen<XA, XB, YA, YB, double, GB, GK>;
       t.grpg32[id][3 * gslot(GB) + gslot(GK)] = &launch_grp_gen<XA, XB, YA, YB, float, GB, GK>;
+      t.flat64[id][3 * gslot(GB) + gslot(GK)] = &launch_flat<XA, XB, YA, YB, GB, GK>;
     }
   }
 }
@@ -219,6 +259,7 @@ void REG_NAME(BRA_CLASS, KET_CLASS)(DispatchTable& t) {
   if constexpr (GRP) {
     t.grp64[id] = &launch_grp<XA, XB, YA, YB, double>;
     t.grp32[id] = &launch_grp<XA, XB, YA, YB, float>;
+    t.flat64[id][0] = &launch_flat<XA, XB, YA, YB, 1, 1>;
   }
   t.grad64[id] = &launch_grad<XA, XB, YA, YB>;
   t.store[id] = &launch_store<XA, XB, YA, YB>;

@@ -68,6 +68,13 @@ struct JKArgs {
   const double* item_m;
   double cutoff, fp32_cut;
   int* queue;                // persistent kernels: the launch's item counter (zeroed before it)
+  // split builds: FP64 quartets listed one per lane (bra position, ket
+  // position), the list length, its capacity, and per bra-group item a flag
+  // set when its FP64 quartets are in the list (the bra-group launch skips it)
+  const int2* flat;
+  const unsigned long long* flat_n;
+  int flat_cap;
+  const int* item_skip;
   const int* ws_atm;         // atm row of each work shell's centre
   double* grad;              // (atm rows, 3)
   // coordinate JVP / Hessian-vector products: directions, (atm rows, 3)
@@ -770,6 +777,7 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R>::value))
   if (lane == 0) item = atomicAdd(args.queue, 1);
   item = __shfl_sync(0xffffffffu, item, 0);
   if (item >= args.nwork) break;
+  if (args.item_skip && args.item_skip[item]) continue;   // its FP64 quartets run from the flat list
   const int4 w = args.work[item];  // (bra-order begin, bra count, ket begin, ket end)
   const double qm = args.split_mode != 0 ? args.item_m[item] : 0.0;
   const double cut = args.cutoff;
@@ -1198,6 +1206,7 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
   if (lane == 0) item = atomicAdd(args.queue, 1);
   item = __shfl_sync(0xffffffffu, item, 0);
   if (item >= args.nwork) break;
+  if (args.item_skip && args.item_skip[item]) continue;   // its FP64 quartets run from the flat list
   const int4 w = args.work[item];  // (bra-order begin, bra count, ket begin, ket end)
   const double qm = args.split_mode != 0 ? args.item_m[item] : 0.0;
   const double cut = args.cutoff;
@@ -1419,6 +1428,73 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
     }
   }
   }  // items
+}
+
+// ---------------------------------------------------------------------------
+// FP64 slice of a split build, for the bra-group items whose FP64 quartets
+// are few (the leading kets of the leading bras, where the bra-group path
+// would keep most lanes of a pass idle): border_kernel lists them as (bra
+// position, ket position) and this kernel gives each lane one quartet, its
+// block in registers and every digested element an atomic add.  Plain lists
+// (GB = GK = 1) and grouped lists, digested as the bra-group kernels do.
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD, int GB, int GK>
+__global__ void __launch_bounds__(128) jk_flat_kernel(JKArgs args) {
+  using CI = ClassInfo<LA, LB, LC, LD>;
+  constexpr int NO = CI::NOUT;
+  const int n = (int)min(*args.flat_n, (unsigned long long)args.flat_cap);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int2 q = args.flat[i];
+    if (q.x < 0) continue;   // space of a reservation that did not fit
+    const BraRec br = load_bra(args, q.x);
+    QuartetGeom g;
+    load_quartet_rec(args, br, q.y, g);
+    const double4* bpp = args.pp_data + g.ppa;
+    const double2* baux = args.pp_aux + g.ppa;
+    if constexpr (GB == 1 && GK == 1) {
+      double out[NO];
+      quartet_block_reg<LA, LB, LC, LD, double>(args, g, bpp, baux, out, nullptr);
+      for (int e = 0; e < args.ndm; ++e) digest_one<LA, LB, LC, LD, double>(args, g, out, e);
+    } else {
+      int aoA[GB], aoB[GB], aoC[GK], aoD[GK];
+      bool bdiag, kdiag;
+      {
+        int4 gx = make_int4(br.ix.z == br.ix.w, 0, 0, 0), gy = make_int4(0, 0, 0, 0);
+        if constexpr (GB > 1) {
+          gx = args.bra_gx[q.x];
+          gy = args.bra_gy[q.x];
+        }
+        const int a4[4] = {br.ix.z, gx.z, gy.x, gy.z}, b4[4] = {br.ix.w, gx.w, gy.y, gy.w};
+#pragma unroll
+        for (int b = 0; b < GB; ++b) { aoA[b] = a4[b]; aoB[b] = b4[b]; }
+        bdiag = gx.x != 0;
+      }
+      {
+        const int4 kix = args.ket_ix[q.y];
+        int4 gx = make_int4(kix.z == kix.w, 0, 0, 0), gy = make_int4(0, 0, 0, 0);
+        if constexpr (GK > 1) {
+          gx = args.ket_gx[q.y];
+          gy = args.ket_gy[q.y];
+        }
+        const int c4[4] = {kix.z, gx.z, gy.x, gy.z}, d4[4] = {kix.w, gx.w, gy.y, gy.w};
+#pragma unroll
+        for (int c = 0; c < GK; ++c) { aoC[c] = c4[c]; aoD[c] = d4[c]; }
+        kdiag = gx.x != 0;
+      }
+      double out[GB * GK * NO];
+      quartet_block_gen<LA, LB, LC, LD, double, GB, GK>(args, g, bpp, baux, args.pp_c + g.ppa, out, nullptr);
+      const double sbk = (bdiag ? 0.5 : 1.0) * (kdiag ? 0.5 : 1.0) * (args.same_list && q.y == q.x ? 0.5 : 1.0);
+#pragma unroll
+      for (int b = 0; b < GB; ++b)
+#pragma unroll
+        for (int c = 0; c < GK; ++c) {
+          QuartetGeom gc = g;
+          gc.aoA = aoA[b]; gc.aoB = aoB[b]; gc.aoC = aoC[c]; gc.aoD = aoD[c];
+          gc.scale = sbk;
+          for (int e = 0; e < args.ndm; ++e) digest_one<LA, LB, LC, LD, double>(args, gc, out + (b * GK + c) * NO, e);
+        }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------

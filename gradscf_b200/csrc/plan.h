@@ -41,6 +41,11 @@ struct DevBuf {
 struct GroupWork {
   int nwork = 0;
   DevBuf work, m;
+  // split builds: the FP64 quartets of items whose FP64 corner is sparse,
+  // one int2 (bra position, ket position) each; the list's length; per item
+  // a flag (its FP64 quartets are in the list)
+  DevBuf flat, flat_n, skip;
+  int flat_cap = 0;
   std::vector<int4> h_items, all_items;
   std::vector<int64_t> item_cost;
   long long quartets = 0, prim_quartets = 0;

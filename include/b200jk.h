@@ -102,6 +102,12 @@ int b200jk_plan_autotune(b200jk_plan* plan, const double* d_density, int32_t nb,
 int b200jk_plan_split_stats(b200jk_plan* plan, void* stream, int64_t* q64, int64_t* q32,
                             int64_t* pq64, int64_t* pq32);
 
+/* After a B200JK_SPLIT call (synchronises `stream`): the FP64 quartets that
+ * ran one per lane from the flat lists (`listed`; list slots, including the
+ * filler of a reservation that did not fit) and the quartets whose
+ * reservation did not fit (`overflow`; they ran on the bra-group path). */
+int b200jk_plan_border_stats(b200jk_plan* plan, void* stream, int64_t* listed, int64_t* overflow);
+
 /* Optional CUDA-event timing of every class-pair launch (on the launching
  * stream).  b200jk_plan_profile synchronises, returns per class pair the
  * summed milliseconds of FP64 and FP32 launches and the launch counts since

@@ -369,3 +369,41 @@ def test_bra_transfer_probe_variants_agree():
     _capi.check(_capi.lib().b200jk_measure_bra_transfer(4096, 2, ns, ctypes.byref(diff), st))
     assert diff.value < 1e-12
     assert ns[0] > 0 and ns[1] > 0
+
+
+def _border_stats(plan):
+    import ctypes
+    lib = _capi.lib()
+    listed, overflow = ctypes.c_int64(), ctypes.c_int64()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _capi.check(lib.b200jk_plan_border_stats(plan._h, st, ctypes.byref(listed), ctypes.byref(overflow)))
+    return listed.value, overflow.value
+
+
+@pytest.mark.parametrize("fp32_cut", [1e-9, 1e-6, 1e-4])
+def test_split_fp64_flat_list_matches_fp64_build(fp32_cut):
+    # (H2O)4 cc-pVDZ (generally contracted s shells: grouped buckets), a
+    # small symmetric density (an SCF increment's scale, so the FP64 quartets
+    # are the leading corners of the work items and run from the flat lists)
+    # and a nonsymmetric one: the two slices of the split build together
+    # against the FP64 build
+    from gradscf_b200 import workloads as W
+    top, par, sa, atm, bas, env = tables(W.water_cluster(4, 1), "cc-pvdz", False)
+    n = top.nao
+    rng = np.random.default_rng(7)
+    d = np.stack([1e-3 * psd_density(n, 20, 5), 1e-3 * rng.standard_normal((n, n)) / n])
+    plan = J.DirectJKPlan([(atm, bas, env)], cart=False, cutoff=1e-12)
+    dd = torch.as_tensor(d.reshape(2, -1), device="cuda")
+    ref = plan.jk_packed(dd, hermi=0).cpu().numpy()
+    out = plan.jk_packed(dd, hermi=0, precision="split", fp32_cut=fp32_cut).cpu().numpy()
+    listed, overflow = _border_stats(plan)
+    assert listed > 0
+    if fp32_cut == 1e-9:
+        # more FP64 quartets than the lists hold: the items whose reservation
+        # did not fit run their FP64 quartets on the bra-group path
+        assert overflow > 0
+    assert np.abs(out - ref).max() < 1e-9, np.abs(out - ref).max()
+    # the symmetric density alone: J and K against the FP64 build
+    ref1 = plan.jk_packed(dd[:1], hermi=1).cpu().numpy()
+    out1 = plan.jk_packed(dd[:1], hermi=1, precision="split", fp32_cut=fp32_cut).cpu().numpy()
+    assert np.abs(out1 - ref1).max() < 1e-9, np.abs(out1 - ref1).max()
