@@ -19,7 +19,7 @@ EXPORTS = (
     "b200jk_plan_quartets", "b200jk_plan_block_offsets", "b200jk_direct_jk",
     "b200jk_check_status", "b200jk_direct_jk_tables", "b200jk_direct_jk_geom_vjp",
     "b200jk_int1e", "b200jk_int1e_grad", "b200jk_plan_class_stats", "b200jk_plan_split_stats",
-    "b200jk_plan_border_stats",
+    "b200jk_plan_border_stats", "b200jk_direct_jk_geom_vjp_precision",
     "b200jk_plan_set_profiling", "b200jk_plan_profile", "b200jk_measure_fma_peak",
     "b200jk_direct_jk_noalloc", "b200jk_graph_create", "b200jk_graph_launch", "b200jk_graph_destroy",
     "b200jk_partition_items", "b200jk_plan_set_shard", "b200jk_plan_autotune",
@@ -74,6 +74,7 @@ def lib():
     h.b200jk_direct_jk_tables.argtypes = [vp, i32, vp, i32, vp, i32, vp, i32, i32, vp, i32, f64,
                                           i32, i32, i32, vp]
     h.b200jk_direct_jk_geom_vjp.argtypes = [vp, vp, i32, vp, i32, i32, vp, vp]
+    h.b200jk_direct_jk_geom_vjp_precision.argtypes = [vp, vp, i32, vp, i32, i32, i32, ctypes.c_double, vp, vp]
     h.b200jk_direct_jk_geom_jvp.argtypes = [vp, vp, i32, i32, vp, vp, i32, i32, vp, vp]
     h.b200jk_direct_jk_geom_hvp.argtypes = [vp, vp, i32, vp, vp, i32, i32, vp, vp]
     h.b200jk_int1e.argtypes = [vp, i32, vp, vp]

@@ -67,7 +67,7 @@ def run_c2(nwater=16, seed=2, npick=6):
         res = S.rhf(mol, conv_tol=1e-12, conv_tol_grad=1e-9, precision=precision, density0=d0)
         e0, e1 = _events()
         e0.record()
-        g = S.rhf_gradient(mol, res)
+        g = S.rhf_gradient(mol, res, precision=precision)   # split: the split-precision VJP too
         e1.record()
         torch.cuda.synchronize()
         grads[precision] = g
@@ -183,6 +183,13 @@ def run_c4(nwater=64, seed=4, cycles=15, quick=False):
             torch.cuda.synchronize()
             out["force_ms"] = e0.elapsed_time(e1)
             out["net_force"] = float(np.abs(g.sum(0)).max())
+            # the same force with the split-precision coordinate VJP
+            e0.record()
+            gs = S.rhf_gradient(mol, res, precision="split")
+            e1.record()
+            torch.cuda.synchronize()
+            out["force_split_vjp_ms"] = e0.elapsed_time(e1)
+            out["force_split_vjp_max_abs_diff"] = float(np.abs(gs - g).max())
     out["split_speedup"] = out["fp64"]["s_per_iter"] / out["split"]["s_per_iter"]
     out["abs_dE_hartree"] = abs(energies["split"] - energies["fp64"])
     return out
@@ -269,10 +276,10 @@ def run_prof(case="jk", nwater=8, basis="cc-pvdz", seed=1):
         cot = torch.stack([d / 2.0, -d / 4.0]).contiguous()
         st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
-        def vjp():
-            _capi.check(lib.b200jk_direct_jk_geom_vjp(plan._h, ctypes.c_void_p(d.data_ptr()), 1,
-                                                      ctypes.c_void_p(cot.data_ptr()), 1, 1,
-                                                      ctypes.c_void_p(g.data_ptr()), st))
+        def vjp(precision=_capi.FP64):
+            _capi.check(lib.b200jk_direct_jk_geom_vjp_precision(
+                plan._h, ctypes.c_void_p(d.data_ptr()), 1, ctypes.c_void_p(cot.data_ptr()), 1, 1, precision,
+                J.DEFAULT_FP32_CUT, ctypes.c_void_p(g.data_ptr()), st))
         vjp()   # first use
         e0, e1 = _events()
         e0.record()
@@ -280,6 +287,14 @@ def run_prof(case="jk", nwater=8, basis="cc-pvdz", seed=1):
         e1.record()
         torch.cuda.synchronize()
         out["vjp_ms"] = e0.elapsed_time(e1)
+        g64 = g.clone()
+        vjp(_capi.SPLIT)
+        e0.record()
+        vjp(_capi.SPLIT)
+        e1.record()
+        torch.cuda.synchronize()
+        out["vjp_split_ms"] = e0.elapsed_time(e1)
+        out["vjp_split_max_abs_diff"] = (g - g64).abs().max().item()
         # per-class launch times of one more VJP (serial launches, CUDA events)
         nc = _capi.NCLASS
         lib.b200jk_plan_set_profiling(plan._h, 1)

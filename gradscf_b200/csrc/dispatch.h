@@ -24,6 +24,7 @@ struct DispatchTable {
   JKLauncher grp64[kQuartetClasses] = {};   // register path over bra groups (null: not built)
   JKLauncher grp32[kQuartetClasses] = {};
   GradLauncher grad64[kQuartetClasses] = {};
+  GradLauncher grad32[kQuartetClasses] = {};   // FP32 slice of a split-precision VJP
   StoreLauncher store[kQuartetClasses] = {};   // packed ERI producer
   SchwarzLauncher schwarz[kPairClasses] = {};
   // grouped-list kernels by (bra, ket) combinations: slot 3*g(gb) + g(gk),

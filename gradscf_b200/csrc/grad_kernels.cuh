@@ -48,7 +48,28 @@ __device__ __forceinline__ double gamma_abcd(const JKArgs& args, long long base,
   return gsum;
 }
 
-template <int LA, int LB, int LC, int LD, int TEAM>
+// Ket range of a coordinate-VJP work item for the requested precision slice
+// (split_mode 1: the kets before the item's FP32 boundary, 2: from it on).
+__device__ __forceinline__ void grad_ket_range(const JKArgs& args, int item, const int4 w, int& kb, int& ke) {
+  kb = w.y;
+  ke = w.z;
+  if (args.split_mode != 0) {
+    const int s = args.split[item];
+    if (args.split_mode == 1) ke = min(ke, s);
+    else kb = max(kb, s);
+  }
+}
+
+// One primitive quartet's scalars in precision R (FP32 quartets: the pair
+// data stored relative to A and C, centre differences formed in FP64).
+template <typename R>
+__device__ __forceinline__ void grad_prim(const JKArgs& args, const QuartetGeom& g, int i, int j, PrimQ<R>& s) {
+  const float3 ac = make_float3(float(g.ax - g.cx), float(g.ay - g.cy), float(g.az - g.cz));
+  prim_any<R>(g, ac, PrimData<R>::a(args, i), PrimData<R>::b(args, i), PrimData<R>::a(args, j),
+              PrimData<R>::b(args, j), s);
+}
+
+template <int LA, int LB, int LC, int LD, int TEAM, typename R>
 __global__ void grad_team_kernel(JKArgs args) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   using GC = GradCfg<LA, LB, LC, LD, TEAM>;
@@ -60,72 +81,72 @@ __global__ void grad_team_kernel(JKArgs args) {
   const int nteams = blockDim.x / TEAM;
   const unsigned mask =
       TEAM == 32 ? 0xffffffffu : (((1u << TEAM) - 1u) << ((threadIdx.x % 32) / TEAM * TEAM));
-  double* G = reinterpret_cast<double*>(smem_raw) + (size_t)team * GC::ELEMS;
-  double* roots = G + 3 * N * NG;
+  R* G = reinterpret_cast<R*>(smem_raw) + (size_t)team * GC::ELEMS;
+  R* roots = G + 3 * N * NG;
   const int4 w = args.work[blockIdx.x];
   const int bra = args.bra_pairs[w.x];
-  for (int k = w.y + team; k < w.z; k += nteams) {
+  int kb, ke;
+  grad_ket_range(args, blockIdx.x, w, kb, ke);
+  for (int k = kb + team; k < ke; k += nteams) {
     QuartetGeom g;
     load_quartet(args, bra, args.ket_pairs[k], g);
     const long long base = args.mol_base[g.mol];
     const int n = args.mol_n[g.mol];
-    double gam[GC::NK];
+    R gam[GC::NK];
     int exps[GC::NK];   // packed exponent digits of (a, b, c, d) per axis
 #pragma unroll
     for (int q = 0; q < GC::NK; ++q) {
       const int o = lane + q * TEAM;
-      gam[q] = 0.0;
+      gam[q] = R(0);
       exps[q] = -1;
       if (o < CI::NOUT) {
         const int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
         const int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
-        gam[q] = g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id);
+        gam[q] = R(g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id));
         exps[q] = ia | (ib << 4) | (ic << 8) | (id << 12);
       }
     }
-    double dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
+    R dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
     for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
-      const double4 P = args.pp_data[i];
-      const double2 PA = args.pp_aux[i];
-      const double alpha = args.pp_exp[i].x, beta = args.pp_exp[i].y;
+      const R alpha = R(args.pp_exp[i].x), beta = R(args.pp_exp[i].y);
       for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
-        PrimQ<double> s;
-        prim_setup<double>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
-        const double gamma_c = args.pp_exp[j].x;
-        for (int f = lane; f < 2 * N; f += TEAM) roots[f] = rys_one<N, double>(s.t, f, args.tb);
+        PrimQ<R> s;
+        grad_prim<R>(args, g, i, j, s);
+        const R gamma_c = R(args.pp_exp[j].x);
+        for (int f = lane; f < 2 * N; f += TEAM) roots[f] = rys_one<N, R>(s.t, f, args.tb);
         __syncwarp(mask);
         for (int tsk = lane; tsk < 3 * N; tsk += TEAM) {
           const int r = tsk / 3, ax = tsk - 3 * r;
-          RootCoef<double> rc;
-          root_coef<double>(s, roots[r], rc);
-          const double abd = ax == 0 ? g.abx : (ax == 1 ? g.aby : g.abz);
-          const double cdd = ax == 0 ? g.cdx : (ax == 1 ? g.cdy : g.cdz);
-          const double g00 = ax == 2 ? roots[N + r] * s.pref : 1.0;
-          build_g<LA + 1, LB + 1, LC + 1, LD, double>(rc.c00[ax], rc.c0p[ax], rc.b10, rc.b01, rc.b00, g00,
-                                                      abd, cdd, G + (r * 3 + ax) * NG);
+          RootCoef<R> rc;
+          root_coef<R>(s, roots[r], rc);
+          const R abd = R(ax == 0 ? g.abx : (ax == 1 ? g.aby : g.abz));
+          const R cdd = R(ax == 0 ? g.cdx : (ax == 1 ? g.cdy : g.cdz));
+          const R g00 = ax == 2 ? roots[N + r] * s.pref : R(1);
+          build_g<LA + 1, LB + 1, LC + 1, LD, R>(rc.c00[ax], rc.c0p[ax], rc.b10, rc.b01, rc.b00, g00, abd, cdd,
+                                                 G + (r * 3 + ax) * NG);
         }
         __syncwarp(mask);
 #pragma unroll
         for (int q = 0; q < GC::NK; ++q) {
-          if (exps[q] < 0 || gam[q] == 0.0) continue;
+          if (exps[q] < 0 || gam[q] == R(0)) continue;
           const int ia = exps[q] & 15, ib = (exps[q] >> 4) & 15, ic = (exps[q] >> 8) & 15, id = exps[q] >> 12;
           const int la[3] = {cart_lx(LA, ia), cart_ly(LA, ia), cart_lz(LA, ia)};
           const int lb[3] = {cart_lx(LB, ib), cart_ly(LB, ib), cart_lz(LB, ib)};
           const int lc[3] = {cart_lx(LC, ic), cart_ly(LC, ic), cart_lz(LC, ic)};
           const int ld[3] = {cart_lx(LD, id), cart_ly(LD, id), cart_lz(LD, id)};
           for (int r = 0; r < N; ++r) {
-            double v[3], fa[3], fb[3], fc[3];
+            R v[3], fa[3], fb[3], fc[3];
 #pragma unroll
             for (int x = 0; x < 3; ++x) {
-              const double* Gx = G + (r * 3 + x) * NG;
+              const R* Gx = G + (r * 3 + x) * NG;
               const int a = la[x], b = lb[x], c = lc[x], d = ld[x];
               v[x] = Gx[GC::idx(a, b, c, d)];
-              fa[x] = 2.0 * alpha * Gx[GC::idx(a + 1, b, c, d)] - (a ? a * Gx[GC::idx(a - 1, b, c, d)] : 0.0);
-              fb[x] = 2.0 * beta * Gx[GC::idx(a, b + 1, c, d)] - (b ? b * Gx[GC::idx(a, b - 1, c, d)] : 0.0);
-              fc[x] = 2.0 * gamma_c * Gx[GC::idx(a, b, c + 1, d)] - (c ? c * Gx[GC::idx(a, b, c - 1, d)] : 0.0);
+              fa[x] = R(2) * alpha * Gx[GC::idx(a + 1, b, c, d)] - (a ? R(a) * Gx[GC::idx(a - 1, b, c, d)] : R(0));
+              fb[x] = R(2) * beta * Gx[GC::idx(a, b + 1, c, d)] - (b ? R(b) * Gx[GC::idx(a, b - 1, c, d)] : R(0));
+              fc[x] = R(2) * gamma_c * Gx[GC::idx(a, b, c + 1, d)] - (c ? R(c) * Gx[GC::idx(a, b, c - 1, d)] : R(0));
             }
-            const double gq = gam[q];
-            const double yz = v[1] * v[2], xz = v[0] * v[2], xy = v[0] * v[1];
+            const R gq = gam[q];
+            const R yz = v[1] * v[2], xz = v[0] * v[2], xy = v[0] * v[1];
             dA[0] += gq * fa[0] * yz; dA[1] += gq * fa[1] * xz; dA[2] += gq * fa[2] * xy;
             dB[0] += gq * fb[0] * yz; dB[1] += gq * fb[1] * xz; dB[2] += gq * fb[2] * xy;
             dC[0] += gq * fc[0] * yz; dC[1] += gq * fc[1] * xz; dC[2] += gq * fc[2] * xy;
@@ -150,10 +171,10 @@ __global__ void grad_team_kernel(JKArgs args) {
       double* gD = args.grad + 3LL * args.ws_atm[g.D];
 #pragma unroll
       for (int x = 0; x < 3; ++x) {
-        atomicAdd(gA + x, dA[x]);
-        atomicAdd(gB + x, dB[x]);
-        atomicAdd(gC + x, dC[x]);
-        atomicAdd(gD + x, -(dA[x] + dB[x] + dC[x]));
+        atomicAdd(gA + x, double(dA[x]));
+        atomicAdd(gB + x, double(dB[x]));
+        atomicAdd(gC + x, double(dC[x]));
+        atomicAdd(gD + x, -(double(dA[x]) + double(dB[x]) + double(dC[x])));
       }
     }
   }
@@ -183,26 +204,29 @@ struct GradBlk {
   static constexpr int NW = (LAB + 1) * (LCD + 1) * (LD + 1);   // recursion scratch per table
   static constexpr int G_OFF = 0, R_OFF = 3 * N * NG, W_OFF = R_OFF + 2 * N, GAM_OFF = W_OFF + 3 * N * NW;
   static constexpr int ELEMS = GAM_OFF + CI::NOUT;
-  static constexpr size_t bytes() { return (size_t)ELEMS * 8; }
+  static constexpr size_t bytes() { return (size_t)ELEMS * 8; }   // FP64; FP32 takes half
   static constexpr bool OK = CI::NOUT > 256 && bytes() <= 220 * 1024;
 };
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(128) grad_block_kernel(JKArgs args) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   using GB = GradBlk<LA, LB, LC, LD>;
   using GC = GradCfg<LA, LB, LC, LD, 1>;
   constexpr int N = GB::N, NG = GB::NG;
-  extern __shared__ __align__(16) double gsm[];
-  double* G = gsm + GB::G_OFF;
-  double* roots = gsm + GB::R_OFF;
-  double* scratch = gsm + GB::W_OFF;
-  double* gam = gsm + GB::GAM_OFF;
+  extern __shared__ __align__(16) unsigned char gsm_raw[];
+  R* gsm = reinterpret_cast<R*>(gsm_raw);
+  R* G = gsm + GB::G_OFF;
+  R* roots = gsm + GB::R_OFF;
+  R* scratch = gsm + GB::W_OFF;
+  R* gam = gsm + GB::GAM_OFF;
   __shared__ double red[9][GB::THREADS / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int4 w = args.work[blockIdx.x];
   const int bra = args.bra_pairs[w.x];
-  for (int k = w.y; k < w.z; ++k) {
+  int kb, ke;
+  grad_ket_range(args, blockIdx.x, w, kb, ke);
+  for (int k = kb; k < ke; ++k) {
     QuartetGeom g;
     load_quartet(args, bra, args.ket_pairs[k], g);
     const long long base = args.mol_base[g.mol];
@@ -210,34 +234,32 @@ __global__ void __launch_bounds__(128) grad_block_kernel(JKArgs args) {
     for (int o = tid; o < CI::NOUT; o += GB::THREADS) {
       const int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
       const int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
-      gam[o] = g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id);
+      gam[o] = R(g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id));
     }
-    double dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
+    R dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
     for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
-      const double4 P = args.pp_data[i];
-      const double2 PA = args.pp_aux[i];
-      const double alpha = args.pp_exp[i].x, beta = args.pp_exp[i].y;
+      const R alpha = R(args.pp_exp[i].x), beta = R(args.pp_exp[i].y);
       for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
-        PrimQ<double> s;
-        prim_setup<double>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
-        const double gamma_c = args.pp_exp[j].x;
+        PrimQ<R> s;
+        grad_prim<R>(args, g, i, j, s);
+        const R gamma_c = R(args.pp_exp[j].x);
         __syncthreads();   // the previous primitive quartet's tables are no longer read
-        if (tid < 2 * N) roots[tid] = rys_one<N, double>(s.t, tid, args.tb);
+        if (tid < 2 * N) roots[tid] = rys_one<N, R>(s.t, tid, args.tb);
         __syncthreads();
         if (tid < 3 * N) {
           const int r = tid / 3, ax = tid - 3 * r;
-          RootCoef<double> rc;
-          root_coef<double>(s, roots[r], rc);
-          const double abd = ax == 0 ? g.abx : (ax == 1 ? g.aby : g.abz);
-          const double cdd = ax == 0 ? g.cdx : (ax == 1 ? g.cdy : g.cdz);
-          const double g00 = ax == 2 ? roots[N + r] * s.pref : 1.0;
-          build_g_mem<LA + 1, LB + 1, LC + 1, LD, double>(rc.c00[ax], rc.c0p[ax], rc.b10, rc.b01, rc.b00, g00, abd,
-                                                         cdd, G + tid * NG, scratch + tid * GB::NW);
+          RootCoef<R> rc;
+          root_coef<R>(s, roots[r], rc);
+          const R abd = R(ax == 0 ? g.abx : (ax == 1 ? g.aby : g.abz));
+          const R cdd = R(ax == 0 ? g.cdx : (ax == 1 ? g.cdy : g.cdz));
+          const R g00 = ax == 2 ? roots[N + r] * s.pref : R(1);
+          build_g_mem<LA + 1, LB + 1, LC + 1, LD, R>(rc.c00[ax], rc.c0p[ax], rc.b10, rc.b01, rc.b00, g00, abd, cdd,
+                                                    G + tid * NG, scratch + tid * GB::NW);
         }
         __syncthreads();
         for (int o = tid; o < CI::NOUT; o += GB::THREADS) {
-          const double gq = gam[o];
-          if (gq == 0.0) continue;
+          const R gq = gam[o];
+          if (gq == R(0)) continue;
           const int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
           const int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
           const int la[3] = {cart_lx(LA, ia), cart_ly(LA, ia), cart_lz(LA, ia)};
@@ -246,17 +268,17 @@ __global__ void __launch_bounds__(128) grad_block_kernel(JKArgs args) {
           const int ld[3] = {cart_lx(LD, id), cart_ly(LD, id), cart_lz(LD, id)};
 #pragma unroll 2
           for (int r = 0; r < N; ++r) {
-            double v[3], fa[3], fb[3], fc[3];
+            R v[3], fa[3], fb[3], fc[3];
 #pragma unroll
             for (int x = 0; x < 3; ++x) {
-              const double* Gx = G + (r * 3 + x) * NG;
+              const R* Gx = G + (r * 3 + x) * NG;
               const int a = la[x], b = lb[x], c = lc[x], d = ld[x];
               v[x] = Gx[GC::idx(a, b, c, d)];
-              fa[x] = 2.0 * alpha * Gx[GC::idx(a + 1, b, c, d)] - (a ? a * Gx[GC::idx(a - 1, b, c, d)] : 0.0);
-              fb[x] = 2.0 * beta * Gx[GC::idx(a, b + 1, c, d)] - (b ? b * Gx[GC::idx(a, b - 1, c, d)] : 0.0);
-              fc[x] = 2.0 * gamma_c * Gx[GC::idx(a, b, c + 1, d)] - (c ? c * Gx[GC::idx(a, b, c - 1, d)] : 0.0);
+              fa[x] = R(2) * alpha * Gx[GC::idx(a + 1, b, c, d)] - (a ? R(a) * Gx[GC::idx(a - 1, b, c, d)] : R(0));
+              fb[x] = R(2) * beta * Gx[GC::idx(a, b + 1, c, d)] - (b ? R(b) * Gx[GC::idx(a, b - 1, c, d)] : R(0));
+              fc[x] = R(2) * gamma_c * Gx[GC::idx(a, b, c + 1, d)] - (c ? R(c) * Gx[GC::idx(a, b, c - 1, d)] : R(0));
             }
-            const double yz = gq * v[1] * v[2], xz = gq * v[0] * v[2], xy = gq * v[0] * v[1];
+            const R yz = gq * v[1] * v[2], xz = gq * v[0] * v[2], xy = gq * v[0] * v[1];
             dA[0] += fa[0] * yz; dA[1] += fa[1] * xz; dA[2] += fa[2] * xy;
             dB[0] += fb[0] * yz; dB[1] += fb[1] * xz; dB[2] += fb[2] * xy;
             dC[0] += fc[0] * yz; dC[1] += fc[1] * xz; dC[2] += fc[2] * xy;
@@ -265,7 +287,8 @@ __global__ void __launch_bounds__(128) grad_block_kernel(JKArgs args) {
       }
     }
     // block reduction of the nine partials; thread 0 adds to the four centres
-    double part[9] = {dA[0], dA[1], dA[2], dB[0], dB[1], dB[2], dC[0], dC[1], dC[2]};
+    double part[9] = {double(dA[0]), double(dA[1]), double(dA[2]), double(dB[0]), double(dB[1]),
+                      double(dB[2]), double(dC[0]), double(dC[1]), double(dC[2])};
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
 #pragma unroll
@@ -310,7 +333,7 @@ struct GradReg {
   static constexpr bool OK = 3 * NGR + CI::NOUT <= B200JK_GRAD_REG_LIMIT;
 };
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(128, 3) grad_reg_kernel(JKArgs args) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   using GC = GradCfg<LA, LB, LC, LD, 1>;
@@ -324,49 +347,49 @@ __global__ void __launch_bounds__(128, 3) grad_reg_kernel(JKArgs args) {
   const int bra = args.bra_pairs[w.x];
   double bA[3] = {0, 0, 0}, bB[3] = {0, 0, 0};
   int atA = 0, atB = 0;
-  for (int k0 = w.y; k0 < w.z; k0 += 32) {
-    const bool active = k0 + lane < w.z;
-    const int k = active ? k0 + lane : w.z - 1;
+  int kb, ke;
+  grad_ket_range(args, item, w, kb, ke);
+  for (int k0 = kb; k0 < ke; k0 += 32) {
+    const bool active = k0 + lane < ke;
+    const int k = active ? k0 + lane : ke - 1;
     QuartetGeom g;
     load_quartet(args, bra, args.ket_pairs[k], g);
     atA = args.ws_atm[g.A];
     atB = args.ws_atm[g.B];
     const long long base = args.mol_base[g.mol];
     const int n = args.mol_n[g.mol];
-    double gam[CI::NOUT];
+    R gam[CI::NOUT];
     static_for<0, CI::NOUT>([&](auto O) {
       constexpr int o = decltype(O)::value;
       constexpr int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
       constexpr int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
-      gam[o] = active ? g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id) : 0.0;
+      gam[o] = active ? R(g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id)) : R(0);
     });
-    double dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
+    R dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
     for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
-      const double4 P = args.pp_data[i];
-      const double2 PA = args.pp_aux[i];
-      const double alpha = args.pp_exp[i].x, beta = args.pp_exp[i].y;
+      const R alpha = R(args.pp_exp[i].x), beta = R(args.pp_exp[i].y);
       for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
-        PrimQ<double> s;
-        prim_setup<double>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
-        const double gamma_c = args.pp_exp[j].x;
-        double x[N], wt[N];
-        rys_roots<N, double>(s.t, x, wt, args.tb);
+        PrimQ<R> s;
+        grad_prim<R>(args, g, i, j, s);
+        const R gamma_c = R(args.pp_exp[j].x);
+        R x[N], wt[N];
+        rys_roots<N, R>(s.t, x, wt, args.tb);
 #pragma unroll
         for (int r = 0; r < N; ++r) {
-          RootCoef<double> rc;
-          root_coef<double>(s, x[r], rc);
-          double G[3][NGR];
-          build_g<LA + 1, LB + 1, LC + 1, LD, double>(rc.c00[0], rc.c0p[0], rc.b10, rc.b01, rc.b00, 1.0, g.abx,
-                                                      g.cdx, G[0]);
-          build_g<LA + 1, LB + 1, LC + 1, LD, double>(rc.c00[1], rc.c0p[1], rc.b10, rc.b01, rc.b00, 1.0, g.aby,
-                                                      g.cdy, G[1]);
-          build_g<LA + 1, LB + 1, LC + 1, LD, double>(rc.c00[2], rc.c0p[2], rc.b10, rc.b01, rc.b00,
-                                                      wt[r] * s.pref, g.abz, g.cdz, G[2]);
+          RootCoef<R> rc;
+          root_coef<R>(s, x[r], rc);
+          R G[3][NGR];
+          build_g<LA + 1, LB + 1, LC + 1, LD, R>(rc.c00[0], rc.c0p[0], rc.b10, rc.b01, rc.b00, R(1), R(g.abx),
+                                                 R(g.cdx), G[0]);
+          build_g<LA + 1, LB + 1, LC + 1, LD, R>(rc.c00[1], rc.c0p[1], rc.b10, rc.b01, rc.b00, R(1), R(g.aby),
+                                                 R(g.cdy), G[1]);
+          build_g<LA + 1, LB + 1, LC + 1, LD, R>(rc.c00[2], rc.c0p[2], rc.b10, rc.b01, rc.b00, wt[r] * s.pref,
+                                                 R(g.abz), R(g.cdz), G[2]);
           static_for<0, CI::NOUT>([&](auto O) {
             constexpr int o = decltype(O)::value;
             constexpr int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
             constexpr int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
-            double v[3], fa[3], fb[3], fc[3];
+            R v[3], fa[3], fb[3], fc[3];
             static_for<0, 3>([&](auto X) {
               constexpr int ax = decltype(X)::value;
               constexpr int a = ax == 0 ? cart_lx(LA, ia) : ax == 1 ? cart_ly(LA, ia) : cart_lz(LA, ia);
@@ -374,15 +397,15 @@ __global__ void __launch_bounds__(128, 3) grad_reg_kernel(JKArgs args) {
               constexpr int c = ax == 0 ? cart_lx(LC, ic) : ax == 1 ? cart_ly(LC, ic) : cart_lz(LC, ic);
               constexpr int d = ax == 0 ? cart_lx(LD, id) : ax == 1 ? cart_ly(LD, id) : cart_lz(LD, id);
               v[ax] = G[ax][GI::idx(a, b, c, d)];
-              fa[ax] = 2.0 * alpha * G[ax][GI::idx(a + 1, b, c, d)];
-              fb[ax] = 2.0 * beta * G[ax][GI::idx(a, b + 1, c, d)];
-              fc[ax] = 2.0 * gamma_c * G[ax][GI::idx(a, b, c + 1, d)];
-              if constexpr (a > 0) fa[ax] -= a * G[ax][GI::idx(a - 1, b, c, d)];
-              if constexpr (b > 0) fb[ax] -= b * G[ax][GI::idx(a, b - 1, c, d)];
-              if constexpr (c > 0) fc[ax] -= c * G[ax][GI::idx(a, b, c - 1, d)];
+              fa[ax] = R(2) * alpha * G[ax][GI::idx(a + 1, b, c, d)];
+              fb[ax] = R(2) * beta * G[ax][GI::idx(a, b + 1, c, d)];
+              fc[ax] = R(2) * gamma_c * G[ax][GI::idx(a, b, c + 1, d)];
+              if constexpr (a > 0) fa[ax] -= R(a) * G[ax][GI::idx(a - 1, b, c, d)];
+              if constexpr (b > 0) fb[ax] -= R(b) * G[ax][GI::idx(a, b - 1, c, d)];
+              if constexpr (c > 0) fc[ax] -= R(c) * G[ax][GI::idx(a, b, c - 1, d)];
             });
-            const double gq = gam[o];
-            const double yz = v[1] * v[2], xz = v[0] * v[2], xy = v[0] * v[1];
+            const R gq = gam[o];
+            const R yz = v[1] * v[2], xz = v[0] * v[2], xy = v[0] * v[1];
             dA[0] += gq * fa[0] * yz; dA[1] += gq * fa[1] * xz; dA[2] += gq * fa[2] * xy;
             dB[0] += gq * fb[0] * yz; dB[1] += gq * fb[1] * xz; dB[2] += gq * fb[2] * xy;
             dC[0] += gq * fc[0] * yz; dC[1] += gq * fc[1] * xz; dC[2] += gq * fc[2] * xy;
@@ -395,10 +418,10 @@ __global__ void __launch_bounds__(128, 3) grad_reg_kernel(JKArgs args) {
       double* gD = args.grad + 3LL * args.ws_atm[g.D];
 #pragma unroll
       for (int x = 0; x < 3; ++x) {
-        atomicAdd(gC + x, dC[x]);
-        atomicAdd(gD + x, -(dA[x] + dB[x] + dC[x]));
-        bA[x] += dA[x];
-        bB[x] += dB[x];
+        atomicAdd(gC + x, double(dC[x]));
+        atomicAdd(gD + x, -(double(dA[x]) + double(dB[x]) + double(dC[x])));
+        bA[x] += double(dA[x]);
+        bB[x] += double(dB[x]);
       }
     }
   }
@@ -435,15 +458,15 @@ struct GradWarp {
   static constexpr int N = GC::NROOT, NGR = GC::NG;
   static constexpr int NGU = CI::NG;                                     // unraised tuples
   static constexpr int NW = (LA + LB + 3) * (LC + LD + 2) * (LD + 1);   // build_g_mem scratch
-  static constexpr int D_OFF = (3 * N * NGR + 1) / 2 * 2;                // 16-byte aligned
+  static constexpr int D_OFF = (3 * N * NGR + 3) / 4 * 4;                // 16-byte aligned in FP32 and FP64
   // the derivative tables overwrite the recursion scratch (dead by then)
   static constexpr int DW = 3 * N * NGU * 4 > 3 * N * NW ? 3 * N * NGU * 4 : 3 * N * NW;
   static constexpr int GAM_OFF = D_OFF + DW;
   static constexpr int R_OFF = GAM_OFF + CI::NOUT;
-  static constexpr int ELEMS = (R_OFF + 2 * N + 1) / 2 * 2;
+  static constexpr int ELEMS = (R_OFF + 2 * N + 3) / 4 * 4;
   static constexpr int WARPS = 4;
   static constexpr int NK = (CI::NOUT + 31) / 32;
-  static constexpr size_t bytes() { return (size_t)WARPS * ELEMS * sizeof(double); }
+  static constexpr size_t bytes() { return (size_t)WARPS * ELEMS * sizeof(double); }   // FP64; FP32 takes half
   // the classes where it beat the team / block kernel, measured per class
   // on (H2O)16 cc-pVTZ (one VJP, serial launches): (21|21) 1.39x, (31|30)
   // 1.61x, (33|10) 1.42x, (30|30) 1.38x, (33|00) 1.30x, (31|20) 1.25x,
@@ -461,19 +484,42 @@ struct GradWarp {
   static constexpr bool OK = PICK && NGU <= 256 && ELEMS * sizeof(double) <= 48 * 1024;
 };
 
-template <int LA, int LB, int LC, int LD>
+// Four derivative-table values (G, f_A, f_B, f_C) stored side by side: one
+// 16-byte access in FP32, two in FP64.
+template <typename R> struct Quad;
+template <> struct Quad<double> {
+  static __device__ __forceinline__ void st(double* p, double a, double b, double c, double d) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(a, b);
+    reinterpret_cast<double2*>(p)[1] = make_double2(c, d);
+  }
+  static __device__ __forceinline__ void ld(const double* p, double& a, double& b, double& c, double& d) {
+    const double2 x = reinterpret_cast<const double2*>(p)[0], y = reinterpret_cast<const double2*>(p)[1];
+    a = x.x; b = x.y; c = y.x; d = y.y;
+  }
+};
+template <> struct Quad<float> {
+  static __device__ __forceinline__ void st(float* p, float a, float b, float c, float d) {
+    *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);
+  }
+  static __device__ __forceinline__ void ld(const float* p, float& a, float& b, float& c, float& d) {
+    const float4 x = *reinterpret_cast<const float4*>(p);
+    a = x.x; b = x.y; c = x.z; d = x.w;
+  }
+};
+
+template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(128) grad_warp_kernel(JKArgs args) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   using GW = GradWarp<LA, LB, LC, LD>;
   using GC = GradCfg<LA, LB, LC, LD, 1>;
   constexpr int N = GW::N, NGR = GW::NGR, NGU = GW::NGU;
-  extern __shared__ __align__(16) double wsm[];
+  extern __shared__ __align__(16) unsigned char wsm_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* G = wsm + warp * GW::ELEMS;
-  double* D = G + GW::D_OFF;
-  double* scratch = D;
-  double* gam = G + GW::GAM_OFF;
-  double* roots = G + GW::R_OFF;
+  R* G = reinterpret_cast<R*>(wsm_raw) + warp * GW::ELEMS;
+  R* D = G + GW::D_OFF;
+  R* scratch = D;
+  R* gam = G + GW::GAM_OFF;
+  R* roots = G + GW::R_OFF;
   // the lane's elements: unraised tuple index per axis, 8 bits each
   int tix[GW::NK];
 #pragma unroll
@@ -491,7 +537,9 @@ __global__ void __launch_bounds__(128) grad_warp_kernel(JKArgs args) {
   }
   const int4 w = args.work[blockIdx.x];
   const int bra = args.bra_pairs[w.x];
-  for (int k = w.y + warp; k < w.z; k += GW::WARPS) {
+  int kb, ke;
+  grad_ket_range(args, blockIdx.x, w, kb, ke);
+  for (int k = kb + warp; k < ke; k += GW::WARPS) {
     QuartetGeom g;
     load_quartet(args, bra, args.ket_pairs[k], g);
     const long long base = args.mol_base[g.mol];
@@ -499,73 +547,70 @@ __global__ void __launch_bounds__(128) grad_warp_kernel(JKArgs args) {
     for (int o = lane; o < CI::NOUT; o += 32) {
       const int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
       const int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
-      gam[o] = g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id);
+      gam[o] = R(g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id));
     }
-    double dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
+    R dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
     for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
-      const double4 P = args.pp_data[i];
-      const double2 PA = args.pp_aux[i];
-      const double alpha = args.pp_exp[i].x, beta = args.pp_exp[i].y;
+      const R alpha = R(args.pp_exp[i].x), beta = R(args.pp_exp[i].y);
       for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
-        PrimQ<double> s;
-        prim_setup<double>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
-        const double gamma_c = args.pp_exp[j].x;
+        PrimQ<R> s;
+        grad_prim<R>(args, g, i, j, s);
+        const R gamma_c = R(args.pp_exp[j].x);
         __syncwarp();   // the previous primitive quartet's tables are no longer read
-        if (lane < 2 * N) roots[lane] = rys_one<N, double>(s.t, lane, args.tb);
+        if (lane < 2 * N) roots[lane] = rys_one<N, R>(s.t, lane, args.tb);
         __syncwarp();
         if (lane < 3 * N) {
           const int r = lane / 3, ax = lane - 3 * r;
-          RootCoef<double> rc;
-          root_coef<double>(s, roots[r], rc);
-          const double abd = ax == 0 ? g.abx : (ax == 1 ? g.aby : g.abz);
-          const double cdd = ax == 0 ? g.cdx : (ax == 1 ? g.cdy : g.cdz);
-          const double g00 = ax == 2 ? roots[N + r] * s.pref : 1.0;
-          build_g_mem<LA + 1, LB + 1, LC + 1, LD, double>(rc.c00[ax], rc.c0p[ax], rc.b10, rc.b01, rc.b00, g00, abd,
-                                                         cdd, G + lane * NGR, scratch + lane * GW::NW);
+          RootCoef<R> rc;
+          root_coef<R>(s, roots[r], rc);
+          const R abd = R(ax == 0 ? g.abx : (ax == 1 ? g.aby : g.abz));
+          const R cdd = R(ax == 0 ? g.cdx : (ax == 1 ? g.cdy : g.cdz));
+          const R g00 = ax == 2 ? roots[N + r] * s.pref : R(1);
+          build_g_mem<LA + 1, LB + 1, LC + 1, LD, R>(rc.c00[ax], rc.c0p[ax], rc.b10, rc.b01, rc.b00, g00, abd, cdd,
+                                                    G + lane * NGR, scratch + lane * GW::NW);
         }
         __syncwarp();
-        const double e2a = 2.0 * alpha, e2b = 2.0 * beta, e2c = 2.0 * gamma_c;
+        const R e2a = R(2) * alpha, e2b = R(2) * beta, e2c = R(2) * gamma_c;
         for (int e = lane; e < 3 * N * NGU; e += 32) {
           const int tbl = e / NGU, tt = e - tbl * NGU;
           const int d = tt % (LD + 1), c = (tt / (LD + 1)) % (LC + 1);
           const int b = (tt / ((LD + 1) * (LC + 1))) % (LB + 1), a = tt / ((LD + 1) * (LC + 1) * (LB + 1));
-          const double* Gt = G + tbl * NGR;
-          const double v = Gt[GC::idx(a, b, c, d)];
-          double fa = e2a * Gt[GC::idx(a + 1, b, c, d)];
-          double fb = e2b * Gt[GC::idx(a, b + 1, c, d)];
-          double fc = e2c * Gt[GC::idx(a, b, c + 1, d)];
-          if (a) fa -= a * Gt[GC::idx(a - 1, b, c, d)];
-          if (b) fb -= b * Gt[GC::idx(a, b - 1, c, d)];
-          if (c) fc -= c * Gt[GC::idx(a, b, c - 1, d)];
-          double2* De = reinterpret_cast<double2*>(D + 4 * e);
-          De[0] = make_double2(v, fa);
-          De[1] = make_double2(fb, fc);
+          const R* Gt = G + tbl * NGR;
+          const R v = Gt[GC::idx(a, b, c, d)];
+          R fa = e2a * Gt[GC::idx(a + 1, b, c, d)];
+          R fb = e2b * Gt[GC::idx(a, b + 1, c, d)];
+          R fc = e2c * Gt[GC::idx(a, b, c + 1, d)];
+          if (a) fa -= R(a) * Gt[GC::idx(a - 1, b, c, d)];
+          if (b) fb -= R(b) * Gt[GC::idx(a, b - 1, c, d)];
+          if (c) fc -= R(c) * Gt[GC::idx(a, b, c - 1, d)];
+          Quad<R>::st(D + 4 * e, v, fa, fb, fc);
         }
         __syncwarp();
-        const double2* D2 = reinterpret_cast<const double2*>(D);
 #pragma unroll
         for (int q = 0; q < GW::NK; ++q) {
           const int o = lane + 32 * q;
           if (o >= CI::NOUT) break;
-          const double gq = gam[o];
-          if (gq == 0.0) continue;
+          const R gq = gam[o];
+          if (gq == R(0)) continue;
           const int tx = tix[q] & 255, ty = (tix[q] >> 8) & 255, tz = tix[q] >> 16;
 #pragma unroll 2
           for (int r = 0; r < N; ++r) {
-            const double2* Dr = D2 + 2 * (3 * r * NGU);
-            const double2 x0 = Dr[2 * tx], x1 = Dr[2 * tx + 1];
-            const double2 y0 = Dr[2 * (NGU + ty)], y1 = Dr[2 * (NGU + ty) + 1];
-            const double2 z0 = Dr[2 * (2 * NGU + tz)], z1 = Dr[2 * (2 * NGU + tz) + 1];
-            const double yz = gq * y0.x * z0.x, xz = gq * x0.x * z0.x, xy = gq * x0.x * y0.x;
-            dA[0] += x0.y * yz; dA[1] += y0.y * xz; dA[2] += z0.y * xy;
-            dB[0] += x1.x * yz; dB[1] += y1.x * xz; dB[2] += z1.x * xy;
-            dC[0] += x1.y * yz; dC[1] += y1.y * xz; dC[2] += z1.y * xy;
+            const R* Dr = D + 4 * (3 * r * NGU);
+            R vx, ax, bx, cx, vy, ay, by, cy, vz, az, bz, cz;
+            Quad<R>::ld(Dr + 4 * tx, vx, ax, bx, cx);
+            Quad<R>::ld(Dr + 4 * (NGU + ty), vy, ay, by, cy);
+            Quad<R>::ld(Dr + 4 * (2 * NGU + tz), vz, az, bz, cz);
+            const R yz = gq * vy * vz, xz = gq * vx * vz, xy = gq * vx * vy;
+            dA[0] += ax * yz; dA[1] += ay * xz; dA[2] += az * xy;
+            dB[0] += bx * yz; dB[1] += by * xz; dB[2] += bz * xy;
+            dC[0] += cx * yz; dC[1] += cy * xz; dC[2] += cz * xy;
           }
         }
       }
     }
     // warp reduction of the nine partials; lane 0 adds to the four centres
-    double part[9] = {dA[0], dA[1], dA[2], dB[0], dB[1], dB[2], dC[0], dC[1], dC[2]};
+    double part[9] = {double(dA[0]), double(dA[1]), double(dA[2]), double(dB[0]), double(dB[1]),
+                      double(dB[2]), double(dC[0]), double(dC[1]), double(dC[2])};
 #pragma unroll
     for (int x = 0; x < 9; ++x)
 #pragma unroll
@@ -602,7 +647,7 @@ struct GradLane {
   static constexpr int NGC = (LA + 1) * (LB + 1) * (LC + 2) * (LD + 1);
   static constexpr int NGMAX = NGA > NGB ? (NGA > NGC ? NGA : NGC) : (NGB > NGC ? NGB : NGC);
   static constexpr int THREADS = 128;
-  static constexpr size_t bytes() { return (size_t)CI::NOUT * THREADS * sizeof(double); }
+  static constexpr size_t bytes() { return (size_t)CI::NOUT * THREADS * sizeof(double); }   // FP64; FP32 half
 #ifndef B200JK_GRAD_LANE_TABLES
 #define B200JK_GRAD_LANE_TABLES 90   // doubles of one centre's three tables
 #endif
@@ -619,28 +664,33 @@ __device__ __forceinline__ double lds_keep(const double* p) {
   asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"((unsigned)__cvta_generic_to_shared(p)));
   return v;
 }
+__device__ __forceinline__ float lds_keep(const float* p) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"((unsigned)__cvta_generic_to_shared(p)));
+  return v;
+}
 
 // d/dX of one centre (X = 0: A, 1: B, 2: C) for every element of the lane's
 // quartet at one root: tables raised in X's index, Gamma from the lane's
 // shared-memory column, partials into d[3].
-template <int LA, int LB, int LC, int LD, int X>
-__device__ __forceinline__ void grad_lane_centre(const RootCoef<double>& rc, double g00, const QuartetGeom& g,
-                                                 double expo, const double* __restrict__ gam, double* d) {
+template <int LA, int LB, int LC, int LD, int X, typename R>
+__device__ __forceinline__ void grad_lane_centre(const RootCoef<R>& rc, R g00, const QuartetGeom& g, R expo,
+                                                 const R* __restrict__ gam, R* d) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   constexpr int RA = LA + (X == 0), RB = LB + (X == 1), RC = LC + (X == 2);
   using GI = GIdx<RA, RB, RC, LD>;
   constexpr int NGX = (RA + 1) * (RB + 1) * (RC + 1) * (LD + 1);
-  double G[3][NGX];
-  build_g<RA, RB, RC, LD, double>(rc.c00[0], rc.c0p[0], rc.b10, rc.b01, rc.b00, 1.0, g.abx, g.cdx, G[0]);
-  build_g<RA, RB, RC, LD, double>(rc.c00[1], rc.c0p[1], rc.b10, rc.b01, rc.b00, 1.0, g.aby, g.cdy, G[1]);
-  build_g<RA, RB, RC, LD, double>(rc.c00[2], rc.c0p[2], rc.b10, rc.b01, rc.b00, g00, g.abz, g.cdz, G[2]);
-  const double e2 = 2.0 * expo;
+  R G[3][NGX];
+  build_g<RA, RB, RC, LD, R>(rc.c00[0], rc.c0p[0], rc.b10, rc.b01, rc.b00, R(1), R(g.abx), R(g.cdx), G[0]);
+  build_g<RA, RB, RC, LD, R>(rc.c00[1], rc.c0p[1], rc.b10, rc.b01, rc.b00, R(1), R(g.aby), R(g.cdy), G[1]);
+  build_g<RA, RB, RC, LD, R>(rc.c00[2], rc.c0p[2], rc.b10, rc.b01, rc.b00, g00, R(g.abz), R(g.cdz), G[2]);
+  const R e2 = R(2) * expo;
   // compile-time element indices: the tables stay in registers
   static_for_n<CI::NOUT>([&](auto O) {
     constexpr int o = decltype(O)::value;
     constexpr int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
     constexpr int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
-    double v[3], f[3];
+    R v[3], f[3];
     static_for_n<3>([&](auto AX) {
       constexpr int ax = decltype(AX)::value;
       constexpr int a = ax == 0 ? cart_lx(LA, ia) : ax == 1 ? cart_ly(LA, ia) : cart_lz(LA, ia);
@@ -650,33 +700,35 @@ __device__ __forceinline__ void grad_lane_centre(const RootCoef<double>& rc, dou
       constexpr int n = X == 0 ? a : X == 1 ? b : c;   // the raised index
       v[ax] = G[ax][GI::idx(a, b, c, dd)];
       f[ax] = e2 * G[ax][GI::idx(a + (X == 0), b + (X == 1), c + (X == 2), dd)];
-      if constexpr (n > 0) f[ax] -= n * G[ax][GI::idx(a - (X == 0), b - (X == 1), c - (X == 2), dd)];
+      if constexpr (n > 0) f[ax] -= R(n) * G[ax][GI::idx(a - (X == 0), b - (X == 1), c - (X == 2), dd)];
     });
-    const double gq = lds_keep(gam + o * GradLane<LA, LB, LC, LD>::THREADS);
+    const R gq = lds_keep(gam + o * GradLane<LA, LB, LC, LD>::THREADS);
     d[0] += gq * f[0] * (v[1] * v[2]);
     d[1] += gq * f[1] * (v[0] * v[2]);
     d[2] += gq * f[2] * (v[0] * v[1]);
   });
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(128) grad_lane_kernel(JKArgs args) {
   using CI = ClassInfo<LA, LB, LC, LD>;
   using GC = GradCfg<LA, LB, LC, LD, 1>;
   using GL = GradLane<LA, LB, LC, LD>;
   constexpr int N = GC::NROOT;
-  extern __shared__ double s_gam[];   // [NOUT][THREADS]
+  extern __shared__ __align__(16) unsigned char s_gam_raw[];   // [NOUT][THREADS]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int item = blockIdx.x * (GL::THREADS / 32) + warp;
   if (item >= args.nwork) return;
-  double* gam = s_gam + threadIdx.x;
+  R* gam = reinterpret_cast<R*>(s_gam_raw) + threadIdx.x;
   const int4 w = args.work[item];
   const int bra = args.bra_pairs[w.x];
   double bA[3] = {0, 0, 0}, bB[3] = {0, 0, 0};
   int atA = 0, atB = 0;
-  for (int k0 = w.y; k0 < w.z; k0 += 32) {
-    const bool active = k0 + lane < w.z;
-    const int k = active ? k0 + lane : w.z - 1;
+  int kb, ke;
+  grad_ket_range(args, item, w, kb, ke);
+  for (int k0 = kb; k0 < ke; k0 += 32) {
+    const bool active = k0 + lane < ke;
+    const int k = active ? k0 + lane : ke - 1;
     QuartetGeom g;
     load_quartet(args, bra, args.ket_pairs[k], g);
     atA = args.ws_atm[g.A];
@@ -687,30 +739,28 @@ __global__ void __launch_bounds__(128) grad_lane_kernel(JKArgs args) {
       const int id = o % CI::ND, ic = (o / CI::ND) % CI::NC;
       const int ib = (o / CI::NCD) % CI::NB, ia = o / (CI::NCD * CI::NB);
       gam[o * GL::THREADS] =
-          active ? g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id) : 0.0;
+          active ? R(g.scale * gamma_abcd(args, base, n, g.aoA + ia, g.aoB + ib, g.aoC + ic, g.aoD + id)) : R(0);
     }
-    double dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
+    R dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
     for (int i = g.ppa; i < g.ppa + g.npa; ++i) {
-      const double4 P = args.pp_data[i];
-      const double2 PA = args.pp_aux[i];
-      const double alpha = args.pp_exp[i].x, beta = args.pp_exp[i].y;
+      const R alpha = R(args.pp_exp[i].x), beta = R(args.pp_exp[i].y);
       for (int j = g.ppc; j < g.ppc + g.npc; ++j) {
-        PrimQ<double> s;
-        prim_setup<double>(g, P, PA, args.pp_data[j], args.pp_aux[j], s);
-        const double gamma_c = args.pp_exp[j].x;
-        double x[N], wt[N];
-        rys_roots<N, double>(s.t, x, wt, args.tb);
+        PrimQ<R> s;
+        grad_prim<R>(args, g, i, j, s);
+        const R gamma_c = R(args.pp_exp[j].x);
+        R x[N], wt[N];
+        rys_roots<N, R>(s.t, x, wt, args.tb);
         // one (root, centre) pass per iteration, not unrolled: one centre's
         // tables are live at a time
 #pragma unroll 1
         for (int tsk = 0; tsk < 3 * N; ++tsk) {
           const int r = tsk / 3, cx = tsk - 3 * r;
-          RootCoef<double> rc;
-          root_coef<double>(s, x[r], rc);
-          const double g00 = wt[r] * s.pref;
-          if (cx == 0) grad_lane_centre<LA, LB, LC, LD, 0>(rc, g00, g, alpha, gam, dA);
-          else if (cx == 1) grad_lane_centre<LA, LB, LC, LD, 1>(rc, g00, g, beta, gam, dB);
-          else grad_lane_centre<LA, LB, LC, LD, 2>(rc, g00, g, gamma_c, gam, dC);
+          RootCoef<R> rc;
+          root_coef<R>(s, x[r], rc);
+          const R g00 = wt[r] * s.pref;
+          if (cx == 0) grad_lane_centre<LA, LB, LC, LD, 0, R>(rc, g00, g, alpha, gam, dA);
+          else if (cx == 1) grad_lane_centre<LA, LB, LC, LD, 1, R>(rc, g00, g, beta, gam, dB);
+          else grad_lane_centre<LA, LB, LC, LD, 2, R>(rc, g00, g, gamma_c, gam, dC);
         }
       }
     }
@@ -719,10 +769,10 @@ __global__ void __launch_bounds__(128) grad_lane_kernel(JKArgs args) {
       double* gD = args.grad + 3LL * args.ws_atm[g.D];
 #pragma unroll
       for (int x = 0; x < 3; ++x) {
-        atomicAdd(gC + x, dC[x]);
-        atomicAdd(gD + x, -(dA[x] + dB[x] + dC[x]));
-        bA[x] += dA[x];
-        bB[x] += dB[x];
+        atomicAdd(gC + x, double(dC[x]));
+        atomicAdd(gD + x, -(double(dA[x]) + double(dB[x]) + double(dC[x])));
+        bA[x] += double(dA[x]);
+        bB[x] += double(dB[x]);
       }
     }
   }

@@ -366,6 +366,38 @@ __global__ void rowmax_kernel(const double* __restrict__ dens, int ndm, long lon
   if (lane == 0) rowmax[row] = v;
 }
 
+// Split-precision coordinate VJP, per Cartesian row i: 8 nb v_i^2 with
+// v_i = max(|D|, 2|Jbar|, 2|Kbar|) over row i and column i of every batch.
+// Each Gamma term of a quartet (ab|cd) is a cotangent element times a
+// density element, each with an index in A, B or C: 8 terms Jbar x D (J_ab
+// D_cd, J_cd D_ab and transposes) and 8 terms Kbar x D per batch, so
+// |Gamma| <= 8 nb max|D| (max|Jbar| + max|Kbar|) <= 8 nb V^2 with V the
+// largest v_i over the rows of A, B and C (the rows the item bound of
+// split_kernel takes).
+__global__ void grad_rowmax_kernel(const double* __restrict__ dens, const double* __restrict__ cj,
+                                   const double* __restrict__ ck, int nb, long long dstride,
+                                   const long long* __restrict__ mol_base, const int* __restrict__ mol_n,
+                                   const int* __restrict__ mol_ao_off, const int* __restrict__ cart_ws,
+                                   const int4* __restrict__ ws_info, int nrows, double* __restrict__ rowmax) {
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= nrows) return;
+  const int m = ws_info[cart_ws[row]].z;
+  const int n = mol_n[m];
+  const long long i = row - mol_ao_off[m];
+  double v = 0.0;
+  for (int e = 0; e < nb; ++e)
+    for (int x = 0; x < 3; ++x) {
+      const double* X = x == 0 ? dens : (x == 1 ? cj : ck);
+      if (!X) continue;
+      const double w = x == 0 ? 1.0 : 2.0;
+      const double* M = X + e * dstride + mol_base[m];
+      for (int j = lane; j < n; j += 32) v = fmax(v, w * fmax(fabs(M[i * n + j]), fabs(M[(long long)j * n + i])));
+    }
+  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+  if (lane == 0) rowmax[row] = 8.0 * nb * v * v;
+}
+
 // Density bound of the quartets of one work item: every density element a
 // quartet (ab|cd) digests (D_cd, D_ab, D_bd, D_bc, D_ad, D_ac) lies in a row
 // of shell A, B or C, so max |D| over those rows bounds them; over the
@@ -2286,10 +2318,20 @@ int b200jk_packed_eri(b200jk_plan* plan, int32_t layout, double* d_out, int64_t 
 int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_t nb,
                               const double* d_cot, int32_t with_j, int32_t with_k, double* d_grad,
                               void* stream) {
+  return b200jk_direct_jk_geom_vjp_precision(plan, d_density, nb, d_cot, with_j, with_k, B200JK_FP64, 0.0, d_grad,
+                                             stream);
+}
+
+int b200jk_direct_jk_geom_vjp_precision(b200jk_plan* plan, const double* d_density, int32_t nb,
+                                        const double* d_cot, int32_t with_j, int32_t with_k, int32_t precision,
+                                        double fp32_cut, double* d_grad, void* stream) {
   return guarded([&] {
     if (!plan || !d_density || !d_cot || !d_grad || nb < 1) invalid("Invalid direct J/K geometry product");
     if ((with_j != 0 && with_j != 1) || (with_k != 0 && with_k != 1) || !(with_j || with_k))
       invalid("Invalid direct J/K geometry product");
+    if (precision != B200JK_FP64 && precision != B200JK_SPLIT) invalid("Unknown precision mode");
+    if (precision == B200JK_SPLIT && !(fp32_cut >= 0 && std::isfinite(fp32_cut))) invalid("Invalid fp32_cut");
+    const bool split = precision == B200JK_SPLIT;
     Plan& p = *plan->p;
     CUDA_OK(cudaSetDevice(p.device));
     cudaStream_t st = (cudaStream_t)stream;
@@ -2309,6 +2351,38 @@ int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_
     if (with_j) to_raw(d_cot, p.d_vj.as<double>());
     if (with_k) to_raw(d_cot + (size_t)(with_j ? nb : 0) * p.out_stride, p.d_vk.as<double>());
     CUDA_OK(cudaMemsetAsync(d_grad, 0, (size_t)p.total_atm * 3 * sizeof(double), st));
+    if (split) {
+      // per item the first ket whose quartets run in FP32: Q_bra Q_ket M_item < fp32_cut
+      // with M_item bounding |Gamma| over the item (grad_rowmax_kernel)
+      const int nrows = (int)(p.d_rowmax.bytes / sizeof(double));
+      grad_rowmax_kernel<<<(nrows + 7) / 8, 256, 0, st>>>(
+          p.d_dens.as<double>(), with_j ? p.d_vj.as<double>() : nullptr, with_k ? p.d_vk.as<double>() : nullptr, nb,
+          p.cart_stride, p.d_mol_base_cart.as<long long>(), p.d_mol_ncart.as<int>(), p.d_mol_ao_off.as<int>(),
+          p.d_cart_ws.as<int>(), p.d_ws_info.as<int4>(), nrows, p.d_rowmax.as<double>());
+      CUDA_OK(cudaGetLastError());
+      for (int c = 0; c < kPairClasses; ++c) {
+        ClassList& L = p.classes[c];
+        const int npos = (int)L.q.size();
+        if (npos == 0) continue;
+        posmax_kernel<<<(npos + 127) / 128, 128, 0, st>>>(L.d_ix.as<int4>(), L.d_gx.as<int4>(), L.d_gy.as<int4>(),
+                                                         L.d_nco.as<int>(), L.d_ra.as<double4>(), npos,
+                                                         ncart_of(pc_la_host(c)), p.d_rowmax.as<double>(),
+                                                         p.d_mol_ao_off.as<int>(), L.d_kmax.as<double>());
+        CUDA_OK(cudaGetLastError());
+      }
+      for (auto* W : p.work) {
+        if (W->nwork == 0) continue;
+        const ClassList& X = p.classes[W->x];
+        const ClassList& Y = p.classes[W->y];
+        const int la = pc_la_host(W->x), lb = W->x - la * (la + 1) / 2;
+        SplitLists L{X.d_ix.as<int4>(), X.d_gx.as<int4>(), X.d_gy.as<int4>(), Y.d_kmax.as<double>(),
+                     X.d_ra.as<double4>(), 1, ncart_of(la), ncart_of(lb)};
+        split_kernel<<<(W->nwork + 3) / 4, 128, 0, st>>>(W->work.as<int4>(), X.d_q.as<double>(), Y.d_q.as<double>(),
+                                                        p.d_rowmax.as<double>(), p.d_mol_ao_off.as<int>(), L,
+                                                        fp32_cut, W->nwork, W->split.as<int>());
+        CUDA_OK(cudaGetLastError());
+      }
+    }
     JKArgs a = base_args(p);
     a.dens = p.d_dens.as<double>();
     a.dstride = p.cart_stride;
@@ -2341,20 +2415,25 @@ int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_
       set_lists(a, p, *W);
       a.work = W->work.as<int4>();
       a.nwork = W->nwork;
-      a.split_mode = 0;
-      ProfileEvent ev{cls, 0, nullptr, nullptr};  // profiling: gradient launches count as FP64
-      if (p.profiling) {
-        CUDA_OK(cudaEventCreate(&ev.start));
-        CUDA_OK(cudaEventCreate(&ev.stop));
-        CUDA_OK(cudaEventRecord(ev.start, ls));
-      }
-      const int rc = disp.grad64[cls](a, ls);
-      if (rc)
-        throw Failure{B200JK_INTERNAL, std::string("gradient launch failed (class pair ") + std::to_string(W->x) + "," +
-                                           std::to_string(W->y) + "): " + cudaGetErrorString((cudaError_t)rc)};
-      if (p.profiling) {
-        CUDA_OK(cudaEventRecord(ev.stop, ls));
-        p.events.push_back(ev);
+      a.split = W->split.as<int>();
+      // FP64 (all kets, or the kets before each item's FP32 boundary), then the FP32 slice
+      for (int slice = 0; slice < (split ? 2 : 1); ++slice) {
+        a.split_mode = split ? slice + 1 : 0;
+        ProfileEvent ev{cls, slice, nullptr, nullptr};
+        if (p.profiling) {
+          CUDA_OK(cudaEventCreate(&ev.start));
+          CUDA_OK(cudaEventCreate(&ev.stop));
+          CUDA_OK(cudaEventRecord(ev.start, ls));
+        }
+        const GradLauncher lg = slice == 0 ? disp.grad64[cls] : disp.grad32[cls];
+        const int rc = lg(a, ls);
+        if (rc)
+          throw Failure{B200JK_INTERNAL, std::string("gradient launch failed (class pair ") + std::to_string(W->x) +
+                                             "," + std::to_string(W->y) + "): " + cudaGetErrorString((cudaError_t)rc)};
+        if (p.profiling) {
+          CUDA_OK(cudaEventRecord(ev.stop, ls));
+          p.events.push_back(ev);
+        }
       }
     }
     if (nstreams > 1)

@@ -146,25 +146,29 @@ int launch_schwarz(const JKArgs& args, int npairs, int cart, cudaStream_t stream
 }
 #endif
 
-template <int LA, int LB, int LC, int LD>
+// The coordinate VJP of one class pair in precision R (FP32: the split
+// slice of small-bound quartets); the kernel family per class is the same
+// in both precisions, shared memory scales with sizeof(R).
+template <int LA, int LB, int LC, int LD, typename R>
 int launch_grad(const JKArgs& args, cudaStream_t stream) {
   if (args.nwork <= 0) return 0;
+  constexpr size_t RS = sizeof(R);
 #ifndef B200JK_GRAD_LANE
 #define B200JK_GRAD_LANE 1
 #endif
   if constexpr (B200JK_GRAD_LANE && GradLane<LA, LB, LC, LD>::OK) {
     // mid-size classes: one lane per quartet, Gamma in shared memory
     using GL = GradLane<LA, LB, LC, LD>;
-    constexpr size_t smem = GL::bytes();
+    constexpr size_t smem = GL::bytes() / 8 * RS;
     static std::atomic<uint64_t> smem_done{0};
-    const cudaError_t ea = smem_opt_in(grad_lane_kernel<LA, LB, LC, LD>, smem, smem_done);
+    const cudaError_t ea = smem_opt_in(grad_lane_kernel<LA, LB, LC, LD, R>, smem, smem_done);
     if (ea != cudaSuccess) return (int)ea;
-    grad_lane_kernel<LA, LB, LC, LD><<<(args.nwork + GL::THREADS / 32 - 1) / (GL::THREADS / 32), GL::THREADS,
-                                       smem, stream>>>(args);
+    grad_lane_kernel<LA, LB, LC, LD, R><<<(args.nwork + GL::THREADS / 32 - 1) / (GL::THREADS / 32), GL::THREADS,
+                                          smem, stream>>>(args);
     return (int)cudaGetLastError();
   }
   if constexpr (GradReg<LA, LB, LC, LD>::OK) {
-    grad_reg_kernel<LA, LB, LC, LD><<<(args.nwork + 3) / 4, 128, 0, stream>>>(args);
+    grad_reg_kernel<LA, LB, LC, LD, R><<<(args.nwork + 3) / 4, 128, 0, stream>>>(args);
     return (int)cudaGetLastError();
   }
 #ifndef B200JK_GRAD_WARP
@@ -173,11 +177,11 @@ int launch_grad(const JKArgs& args, cudaStream_t stream) {
   if constexpr (B200JK_GRAD_WARP && GradWarp<LA, LB, LC, LD>::OK) {
     // the classes between: one warp per quartet, derivative tables in shared memory
     using GW = GradWarp<LA, LB, LC, LD>;
-    constexpr size_t smem = GW::bytes();
+    constexpr size_t smem = GW::bytes() / 8 * RS;
     static std::atomic<uint64_t> smem_done{0};
-    const cudaError_t ea = smem_opt_in(grad_warp_kernel<LA, LB, LC, LD>, smem, smem_done);
+    const cudaError_t ea = smem_opt_in(grad_warp_kernel<LA, LB, LC, LD, R>, smem, smem_done);
     if (ea != cudaSuccess) return (int)ea;
-    grad_warp_kernel<LA, LB, LC, LD><<<args.nwork, 32 * GW::WARPS, smem, stream>>>(args);
+    grad_warp_kernel<LA, LB, LC, LD, R><<<args.nwork, 32 * GW::WARPS, smem, stream>>>(args);
     return (int)cudaGetLastError();
   }
 #ifndef B200JK_GRAD_BLOCK
@@ -186,23 +190,24 @@ int launch_grad(const JKArgs& args, cudaStream_t stream) {
   if constexpr (B200JK_GRAD_BLOCK && GradBlk<LA, LB, LC, LD>::OK) {
     // large classes: one quartet per block at a time (block-wide teams)
     using GB = GradBlk<LA, LB, LC, LD>;
-    constexpr size_t smem = GB::bytes();
+    constexpr size_t smem = GB::bytes() / 8 * RS;
     static std::atomic<uint64_t> smem_done{0};
-    const cudaError_t ea = smem_opt_in(grad_block_kernel<LA, LB, LC, LD>, smem, smem_done);
+    const cudaError_t ea = smem_opt_in(grad_block_kernel<LA, LB, LC, LD, R>, smem, smem_done);
     if (ea != cudaSuccess) return (int)ea;
-    grad_block_kernel<LA, LB, LC, LD><<<args.nwork, GB::THREADS, smem, stream>>>(args);
+    grad_block_kernel<LA, LB, LC, LD, R><<<args.nwork, GB::THREADS, smem, stream>>>(args);
     return (int)cudaGetLastError();
   }
   using CI = ClassInfo<LA, LB, LC, LD>;
   constexpr int TEAM = CI::NOUT <= 8 ? 4 : CI::NOUT <= 64 ? 8 : CI::NOUT <= 256 ? 16 : 32;
   using GC = GradCfg<LA, LB, LC, LD, TEAM>;
-  constexpr size_t per_team = GC::bytes();
+  constexpr size_t per_team = GC::bytes() / 8 * RS;
   int teams = 128 / TEAM;
   while (teams > 1 && per_team * teams > 200 * 1024) --teams;
   const size_t smem = per_team * teams;
   static std::atomic<uint64_t> smem_done{0};
-  smem_opt_in(grad_team_kernel<LA, LB, LC, LD, TEAM>, smem, smem_done);
-  grad_team_kernel<LA, LB, LC, LD, TEAM><<<args.nwork, teams * TEAM, smem, stream>>>(args);
+  const cudaError_t ea = smem_opt_in(grad_team_kernel<LA, LB, LC, LD, TEAM, R>, smem, smem_done);
+  if (ea != cudaSuccess) return (int)ea;
+  grad_team_kernel<LA, LB, LC, LD, TEAM, R><<<args.nwork, teams * TEAM, smem, stream>>>(args);
   return (int)cudaGetLastError();
 }
 
@@ -261,7 +266,8 @@ void REG_NAME(BRA_CLASS, KET_CLASS)(DispatchTable& t) {
     t.grp32[id] = &launch_grp<XA, XB, YA, YB, float>;
     t.flat64[id][0] = &launch_flat<XA, XB, YA, YB, 1, 1>;
   }
-  t.grad64[id] = &launch_grad<XA, XB, YA, YB>;
+  t.grad64[id] = &launch_grad<XA, XB, YA, YB, double>;
+  t.grad32[id] = &launch_grad<XA, XB, YA, YB, float>;
   t.store[id] = &launch_store<XA, XB, YA, YB>;
   t.reg_path[id] = Policy<XA, XB, YA, YB, float>::REG || Policy<XA, XB, YA, YB>::REG;
   t.tile[id] = Policy<XA, XB, YA, YB>::TILE;

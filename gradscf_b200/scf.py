@@ -20,7 +20,7 @@ import torch
 
 from . import _capi
 from .basis import nuclear_repulsion, nuclear_repulsion_gradient, pack, prepare_basis
-from .jk import DEFAULT_FP32_CUT, DirectJKPlan
+from .jk import DEFAULT_FP32_CUT, PRECISIONS, DirectJKPlan
 
 
 @dataclass
@@ -167,13 +167,15 @@ def rhf(mol: Molecule, *, conv_tol=1e-10, conv_tol_grad=None, max_cycle=100, pre
                      mo_energy=mo_e, mo_coeff=c, nocc=nocc, jk_ms=times, energies=energies)
 
 
-def rhf_gradient(mol: Molecule, res: SCFResult):
+def rhf_gradient(mol: Molecule, res: SCFResult, *, precision="fp64", fp32_cut=DEFAULT_FP32_CUT):
     """Nuclear gradient dE/dR (natom, 3) of a converged RHF result.
 
     One-electron terms (D-weighted h derivatives incl. the operator
     derivative, W-weighted overlap derivatives) and the two-electron J/K
     coordinate VJP with cotangents J* = D/2, K* = -D/4, then the centre
     rows folded onto their nuclei, plus the nuclear repulsion gradient.
+    precision="split" runs the VJP's small-bound quartets in FP32
+    (b200jk_direct_jk_geom_vjp_precision).
     """
     dev = mol.device
     d = res.density
@@ -190,9 +192,9 @@ def rhf_gradient(mol: Molecule, res: SCFResult):
         _capi.check(lib.b200jk_int1e_grad(mol.plan._h, ctypes.c_void_p(dd.data_ptr()),
                                           ctypes.c_void_p(ww.data_ptr()), ctypes.c_void_p(g1.data_ptr()), st))
         cot = torch.stack([d / 2.0, -d / 4.0]).reshape(2, 1, -1).contiguous()
-        _capi.check(lib.b200jk_direct_jk_geom_vjp(mol.plan._h, ctypes.c_void_p(dd.data_ptr()), 1,
-                                                  ctypes.c_void_p(cot.data_ptr()), 1, 1,
-                                                  ctypes.c_void_p(g2.data_ptr()), st))
+        _capi.check(lib.b200jk_direct_jk_geom_vjp_precision(
+            mol.plan._h, ctypes.c_void_p(dd.data_ptr()), 1, ctypes.c_void_p(cot.data_ptr()), 1, 1,
+            PRECISIONS[precision], float(fp32_cut), ctypes.c_void_p(g2.data_ptr()), st))
     mol.plan.reduce_shards(g2)   # sharded plan: sum the ranks' two-electron parts
     g = (g1 + g2).cpu().numpy()
     nnuc = len(mol.charges)

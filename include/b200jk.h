@@ -225,6 +225,16 @@ int b200jk_direct_jk_geom_vjp(b200jk_plan* plan, const double* d_density, int32_
                               const double* d_cot, int32_t with_j, int32_t with_k, double* d_grad,
                               void* stream);
 
+/* The same VJP in split precision (precision = B200JK_SPLIT): per work item,
+ * the quartets with Q_bra Q_ket M < fp32_cut run in FP32, M = 8 nb
+ * max(|D|, 2|Jbar|, 2|Kbar|)^2 over the rows and columns of the item's A, B
+ * and C shells (a bound on |Gamma|); the rest, and every accumulation across
+ * quartets, in FP64.  B200JK_FP64 is b200jk_direct_jk_geom_vjp.  No reference
+ * counterpart (the reference's VJP is FP64). */
+int b200jk_direct_jk_geom_vjp_precision(b200jk_plan* plan, const double* d_density, int32_t nb,
+                                        const double* d_cot, int32_t with_j, int32_t with_k, int32_t precision,
+                                        double fp32_cut, double* d_grad, void* stream);
+
 /* Coordinate JVP of J/K (replaces gradscf_direct_jk_geometry_jvp_cpu_v1 with
  * order 1 and 2, csrc/direct_jk_geometry.cc:8-99):
  *   d_v == NULL : d_out = d/du (J, K)           (order 1)

@@ -118,3 +118,18 @@ def test_uhf_doublet_on_stacked_alpha_beta_builds_vs_oracle():
                               cart=False, workers=8)
     assert np.abs(j.cpu().numpy() - j0.sum(0)).max() < 1e-10
     assert np.abs(ka.cpu().numpy() - k0[0]).max() < 1e-10 and np.abs(kb.cpu().numpy() - k0[1]).max() < 1e-10
+
+
+def test_split_precision_vjp_matches_fp64():
+    # (H2O)3 cc-pVTZ (f shells: every VJP kernel family), converged RHF density:
+    # the FP64 slice alone (cut 0) is the FP64 VJP; FP32 slices stay close
+    from gradscf_b200 import workloads as W
+    mol = S.Molecule(W.water_cluster(3, 2), "cc-pvtz", cart=False, schwarz_cut=1e-12)
+    res = S.rhf(mol, conv_tol=1e-9)
+    g64 = S.rhf_gradient(mol, res)
+    g0 = S.rhf_gradient(mol, res, precision="split", fp32_cut=0.0)
+    assert np.abs(g0 - g64).max() < 1e-12
+    for cut, tol in ((1e-6, 1e-8), (1e-3, 1e-6)):
+        gs = S.rhf_gradient(mol, res, precision="split", fp32_cut=cut)
+        err = np.abs(gs - g64).max()
+        assert 0.0 < err < tol, (cut, err)
