@@ -170,8 +170,10 @@ extern "C" int b200jk_packed_jk(const double* d_eri, int32_t layout, int64_t eri
       e = cudaMemsetAsync(jp, 0, (size_t)nb * np * sizeof(double), st);
       if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
     }
+    // the attribute is set once per device, to the largest size any call asks for
     static std::atomic<uint64_t> smem_done{0};
-    b200jk::smem_opt_in(b200jk::packed_jk_kernel, smem, smem_done);
+    e = b200jk::smem_opt_in(b200jk::packed_jk_kernel, smem > 48 * 1024 ? (size_t)200 * 1024 : smem, smem_done);
+    if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
     b200jk::packed_jk_kernel<<<(unsigned)np, 32, smem, st>>>(d_eri, layout, n, np, d_density, nb, d_out, jp,
                                                             with_j, with_k);
     e = cudaGetLastError();

@@ -407,3 +407,18 @@ def test_split_fp64_flat_list_matches_fp64_build(fp32_cut):
     ref1 = plan.jk_packed(dd[:1], hermi=1).cpu().numpy()
     out1 = plan.jk_packed(dd[:1], hermi=1, precision="split", fp32_cut=fp32_cut).cpu().numpy()
     assert np.abs(out1 - ref1).max() < 1e-9, np.abs(out1 - ref1).max()
+
+
+def test_packed_jk_growing_batches_keep_shared_memory_limit():
+    # the consumer's per-row exchange sums take 32 n nb bytes of shared memory:
+    # a 60 KB call, then a 150 KB one in the same process (the kernel's
+    # shared-memory limit is set once per device, for the largest size)
+    top, par, sa, atm, bas, env = tables(WATER, "cc-pvtz", False)   # n = 58
+    s8 = J.packed_eri(atm, bas, env, cart=False, aosym="s8")
+    rng = np.random.default_rng(11)
+    d = torch.as_tensor(rng.normal(size=(84, top.nao, top.nao)), device="cuda")
+    j1, k1 = J.packed_jk(s8, d[:1])
+    for nb in (33, 84):
+        j, k = J.packed_jk(s8, d[:nb])
+        assert torch.abs(j[0] - j1[0]).max().item() < 1e-12
+        assert torch.abs(k[0] - k1[0]).max().item() < 1e-12
