@@ -101,10 +101,17 @@ int launch_grp(const JKArgs& args, cudaStream_t stream) {
 template <int LA, int LB, int LC, int LD, typename R, int GB, int GK>
 int launch_grp_gen(const JKArgs& args, cudaStream_t stream) {
   if (args.nwork <= 0) return 0;
+  constexpr size_t smem = (size_t)kRegWarps * GrpGenAcc<LA, LB, LC, LD, GB, GK>::N * 32 * sizeof(R);
+  // static caches plus these pass sums pass 48 KB for most buckets: opt in
+  // (to at least 64 KB of dynamic shared memory) for every one
+  static std::atomic<uint64_t> smem_done{0};
+  const cudaError_t ea =
+      smem_opt_in(jk_grp_gen_kernel<LA, LB, LC, LD, R, GB, GK>, std::max(smem, (size_t)64 * 1024), smem_done);
+  if (ea != cudaSuccess) return (int)ea;
   static std::atomic<int> resident[64];
-  const int wave = persistent_blocks(jk_grp_gen_kernel<LA, LB, LC, LD, R, GB, GK>, 32 * kRegWarps, 0, resident);
+  const int wave = persistent_blocks(jk_grp_gen_kernel<LA, LB, LC, LD, R, GB, GK>, 32 * kRegWarps, smem, resident);
   const int blocks = std::min((args.nwork + kRegWarps - 1) / kRegWarps, wave);
-  jk_grp_gen_kernel<LA, LB, LC, LD, R, GB, GK><<<blocks, 32 * kRegWarps, 0, stream>>>(args);
+  jk_grp_gen_kernel<LA, LB, LC, LD, R, GB, GK><<<blocks, 32 * kRegWarps, smem, stream>>>(args);
   return (int)cudaGetLastError();
 }
 
@@ -243,9 +250,16 @@ void register_gen(DispatchTable& t, int id) {
   if constexpr (GROUPED && okb && okk && !(GB == 1 && GK == 1)) {
     t.jkg64[id][3 * gslot(GB) + gslot(GK)] = &launch_gen<XA, XB, YA, YB, double, GB, GK>;
     t.jkg32[id][3 * gslot(GB) + gslot(GK)] = &launch_gen<XA, XB, YA, YB, float, GB, GK>;
-    // pass sums (N x 32 lanes x 4 warps) beside the FP64 primitive and
-    // coefficient caches (20 KB) within 48 KB of static shared memory
-    if constexpr (GRP_GEN && GrpGenAcc<XA, XB, YA, YB, GB, GK>::N <= 26) {
+    // pass sums (N x 32 lanes x 4 warps, dynamic shared memory: 64 KB in FP64
+    // at N = 64) beside the primitive and coefficient caches.  Measured on
+    // (H2O)32 cc-pVDZ: buckets with up to 2 ket combinations gain from the
+    // bra-group path up to N = 64 ((10|10), (11|10), (20|10): 3-8%); with 4
+    // ket combinations ((l0|00) classes) it was 30-48% slower above N = 26
+#ifndef B200JK_GRP_GEN_N
+#define B200JK_GRP_GEN_N 64
+#endif
+    constexpr int NACC = GrpGenAcc<XA, XB, YA, YB, GB, GK>::N;
+    if constexpr (GRP_GEN && (NACC <= 26 || (GK <= 2 && NACC <= B200JK_GRP_GEN_N))) {
       t.grpg64[id][3 * gslot(GB) + gslot(GK)] = &launch_grp_gen<XA, XB, YA, YB, double, GB, GK>;
       t.grpg32[id][3 * gslot(GB) + gslot(GK)] = &launch_grp_gen<XA, XB, YA, YB, float, GB, GK>;
       t.flat64[id][3 * gslot(GB) + gslot(GK)] = &launch_flat<XA, XB, YA, YB, GB, GK>;

@@ -1218,7 +1218,10 @@ __global__ void __launch_bounds__(128, (RegMinBlocks<LA, LB, LC, LD, R,
   __shared__ PA_t s_pp[kRegWarps][kBraPrimCache];
   __shared__ PB_t s_aux[kRegWarps][kBraPrimCache];
   __shared__ C4 s_co[kRegWarps][kBraPrimCache];
-  __shared__ R s_acc[kRegWarps][GA::N <= 26 ? GA::N : 1][32];
+  // the pass sums (GA::N values of 32 lanes per warp) in dynamic shared
+  // memory, sized by the launcher
+  extern __shared__ __align__(16) unsigned char s_acc_raw[];
+  R(*s_acc)[GA::N][32] = reinterpret_cast<R(*)[GA::N][32]>(s_acc_raw);
   constexpr bool kSharedBoys = sizeof(R) == 4 && CI::NROOT <= 3;
   __shared__ __align__(16) float s_boys[kSharedBoys ? 401 * 8 : 4];
   if constexpr (kSharedBoys) {
