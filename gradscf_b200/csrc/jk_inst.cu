@@ -250,16 +250,12 @@ void register_gen(DispatchTable& t, int id) {
   if constexpr (GROUPED && okb && okk && !(GB == 1 && GK == 1)) {
     t.jkg64[id][3 * gslot(GB) + gslot(GK)] = &launch_gen<XA, XB, YA, YB, double, GB, GK>;
     t.jkg32[id][3 * gslot(GB) + gslot(GK)] = &launch_gen<XA, XB, YA, YB, float, GB, GK>;
-    // pass sums (N x 32 lanes x 4 warps, dynamic shared memory: 64 KB in FP64
-    // at N = 64) beside the primitive and coefficient caches.  Measured on
-    // (H2O)32 cc-pVDZ: buckets with up to 2 ket combinations gain from the
-    // bra-group path up to N = 64 ((10|10), (11|10), (20|10): 3-8%); with 4
-    // ket combinations ((l0|00) classes) it was 30-48% slower above N = 26
-#ifndef B200JK_GRP_GEN_N
-#define B200JK_GRP_GEN_N 64
-#endif
+    // pass sums (N x 32 lanes x 4 warps) in dynamic shared memory.  Up to 26
+    // per lane: wider buckets measured 3-8% faster in the FP32 slices with up
+    // to 2 ket combinations but 30-48% slower with 4, and the (H2O)64 cc-pVTZ
+    // FP64 build 8% slower (11.9 -> 12.9 s), so they keep the per-quartet form
     constexpr int NACC = GrpGenAcc<XA, XB, YA, YB, GB, GK>::N;
-    if constexpr (GRP_GEN && (NACC <= 26 || (GK <= 2 && NACC <= B200JK_GRP_GEN_N))) {
+    if constexpr (GRP_GEN && NACC <= 26) {
       t.grpg64[id][3 * gslot(GB) + gslot(GK)] = &launch_grp_gen<XA, XB, YA, YB, double, GB, GK>;
       t.grpg32[id][3 * gslot(GB) + gslot(GK)] = &launch_grp_gen<XA, XB, YA, YB, float, GB, GK>;
       t.flat64[id][3 * gslot(GB) + gslot(GK)] = &launch_flat<XA, XB, YA, YB, GB, GK>;
